@@ -1,0 +1,363 @@
+"""Benchmark of the batched VBD time step (one JSON line on rank 0).
+
+Workload (default, "batched"): 256 seeded beam scenes, hex-grid dims nx in [4, 96],
+ny, nz in [2, 24] (cell edge 1/16 m), element type uniform over {P1 tet (6-tet split),
+P2 tet, Q1 hex}, E log-uniform in [1e4, 1e7] Pa, nu uniform in [0.30, 0.49], rho = 1000,
+stable Neo-Hookean, x = 0 face fixed, gravity -z, each scene with its own DSAT colouring;
+one step = one 1/60 s frame of 4 sub-steps x 20 VBD iterations over all scenes, batched
+mixed precision (one launch per element type and colour, the sub-step as a CUDA graph).
+Synthetic data; the state (~1 GB) is larger than L2, so no flush is needed between steps.
+
+metric: vertex-iterations/s = sum over scenes of free nodes x iterations x sub-steps per
+step, / time.  Also reported: the plain single-scene drop-in path (each scene stepped on
+its own, FP32, one launch per colour, no graph) on the same scenes and GPU, p50/p99 step
+latency, the end-to-end number through the C ABI with host buffers, the roofline of the
+dominant kernel, and the reference CPU VBD path timed on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload batched|p2|cfg1]
+"""
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FRAME_DT = 1.0 / 60.0
+
+
+def workload_specs(name, seed):
+    """List of scene specs: (element, cells, size, young, poisson, density, gravity, iterations, substeps, dt)."""
+    import octopusengine_b200 as ob
+    rng = np.random.default_rng(seed)
+    specs = []
+    if name == "batched":
+        for _ in range(256):
+            nx, ny, nz = int(rng.integers(4, 97)), int(rng.integers(2, 25)), int(rng.integers(2, 25))
+            e = [ob.TETRA, ob.TETRA10, ob.HEXA][int(rng.integers(0, 3))]
+            young = float(np.exp(rng.uniform(np.log(1e4), np.log(1e7))))
+            nu = float(rng.uniform(0.30, 0.49))
+            specs.append(dict(element=e, cells=(nx, ny, nz), size=(nx / 16.0, ny / 16.0, nz / 16.0), young=young,
+                              poisson=nu, density=1000.0))
+        return specs, 20, 4, FRAME_DT
+    if name == "p2":   # config 2: P2 beam 64x16x16 over 4x1x1 m, E=1e6, nu=0.49, rho=1100
+        return [dict(element=ob.TETRA10, cells=(64, 16, 16), size=(4.0, 1.0, 1.0), young=1e6, poisson=0.49,
+                     density=1100.0, v0_sigma=0.05)], 10, 5, FRAME_DT
+    if name == "cfg1":  # config 1: 8x2x2 P1 beam, E=1e5, nu=0.45, dt=0.01, 1 x 20
+        return [dict(element=ob.TETRA, cells=(8, 2, 2), size=(1.0, 0.25, 0.25), young=1e5, poisson=0.45,
+                     density=1000.0)], 20, 1, 0.01
+    raise SystemExit("unknown workload " + name)
+
+
+def build_scene(ctx, spec, iterations, precision, seed):
+    import octopusengine_b200 as ob
+    X, T = ob.beam_mesh(spec["element"], spec["cells"], spec["size"])
+    fixed = ob.fixed_by_plane(X, (0.01, 0.0, 0.0), (-1.0, 0.0, 0.0))
+    kw = dict(density=spec["density"], mass_distribution=ob.MASS_FEMSHAPE, material=ob.STABLE_NEOHOOKE,
+              young=spec["young"], poisson=spec["poisson"], fixed_ids=fixed, iterations=iterations,
+              gravity=(0.0, 0.0, -9.81), precision=precision)
+    if spec.get("v0_sigma"):
+        kw["initial_velocity"] = np.random.default_rng(seed).normal(0, spec["v0_sigma"], X.shape).astype(np.float32)
+    return ob.Scene(ctx, spec["element"], X, T, **kw)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % device)
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().split("\n") if r.strip()]
+            sm = [float(r[1]) for r in rows]
+            out["sm_mhz"] = float(np.median(sm))
+            out["sm_max_mhz"] = float(rows[0][2])
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for k, n in enumerate(names):
+                if any(r[5 + k].strip() == "Active" for r in rows):
+                    out["reasons"].append(n)
+            out["samples"] = len(rows)
+            out["power_w_max"] = max(float(r[3]) for r in rows)
+        except Exception:
+            pass
+        return out
+
+
+def cpu_reference(specs, iterations, substeps, dt, threads, sample_every, sample_iters):
+    """The reference CPU VBD (single-thread Gauss-Seidel per scene, as shipped, with its
+    per-iteration force pass) over a sample of the workload's scenes, scenes spread over
+    the host threads.  Returns vertex-iterations/s and the sample description."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    import octopusengine_b200 as ob
+    sel = specs[::sample_every]
+    keep, solvers, vit = [], [], 0
+    for sp in sel:
+        X, T = O.beam_mesh(sp["element"], sp["cells"], sp["size"])
+        m = O.masses(sp["element"], X, T, sp["density"], 1)
+        fixed = O.fixed_by_plane(X, (0.01, 0, 0), (-1, 0, 0))
+        s = O.Scene(sp["element"], X, T, m, young=sp["young"], poisson=sp["poisson"], fixed=fixed,
+                    iterations=sample_iters, gravity=(0, 0, -9.81))
+        keep.append(s)
+        solvers.append(O.CpuVBD(s))
+        vit += (len(X) - len(fixed)) * sample_iters
+    secs = O.run_cpu_many(solvers, dt, 1, True, threads)
+    desc = ("%d of %d scenes (every %d-th), 1 sub-step x %d iterations of dt=%.5f s, %d host threads, "
+            "reference CPU VBD restated in C++ (oracle/), per-iteration force pass included"
+            % (len(sel), len(specs), sample_every, sample_iters, dt / substeps, threads))
+    return vit / secs, secs, desc
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "p2", "cfg1"])
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    specs, iterations, substeps, frame_dt = workload_specs(args.workload, args.seed)
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        every = 4 if args.workload == "batched" else 1
+        its = 4 if args.workload == "batched" else (2 if args.workload == "p2" else iterations)
+        vals = []
+        for _ in range(args.warmup + args.steps):
+            v, secs, desc = cpu_reference(specs, iterations, substeps, frame_dt / substeps * substeps, threads, every, its)
+            vals.append(v)
+        v = float(np.median(vals[args.warmup:]))
+        line = {"impl": "reference", "metric": "vertex_iterations_per_s", "value": v, "unit": "vertex-iter/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": args.workload, "scenes": len(specs), "seed": args.seed},
+                "cpu_baseline": {"value": v, "unit": "vertex-iter/s", "cores": threads, "kind": "port",
+                                 "sample": desc},
+                "e2e": {"value": v, "unit": "vertex-iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    device = local
+    torch.cuda.set_device(device)
+    import octopusengine_b200 as ob
+    from octopusengine_b200 import capi
+    import ctypes as C
+
+    ctx = ob.Context(device, 0)
+    # scene set-up (host colouring etc.) in parallel host threads
+    t0 = time.time()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        scenes = list(ex.map(lambda a: build_scene(ctx, a[1], iterations, ob.PREC_MIXED, args.seed + a[0]),
+                             enumerate(specs)))
+    setup_s = time.time() - t0
+    batch = ob.Batch(ctx, scenes)
+    free_nodes = sum(s.n_nodes - s.n_fixed for s in scenes)
+    vit_per_step = free_nodes * iterations * substeps
+
+    stream_ptr = C.c_void_p()
+    capi.lib().oct_ctx_stream(ctx.handle, C.byref(stream_ptr))
+    stream = torch.cuda.ExternalStream(stream_ptr.value, device=device)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(args.warmup):
+        batch.step(frame_dt, substeps)
+    torch.cuda.synchronize()
+
+    # ---- timed region: K batched steps, per-step events on the library's stream
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    launches0 = ctx.launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(device) as clocks:
+        ev[0].record(stream)
+        for k in range(args.steps):
+            batch.step(frame_dt, substeps)
+            ev[k + 1].record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    launches = ctx.launch_count() - launches0
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = vit_per_step * args.steps * world / (total_ms * 1e-3)
+
+    # ---- end to end through the C ABI with pinned host buffers
+    n_state = batch.state_size
+    host = torch.empty(n_state, dtype=torch.float32, pin_memory=True)
+    host_np = host.numpy()
+    batch.get_state(host_np)
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e_start.record(stream)
+    for _ in range(args.steps):
+        batch.set_state(host_np)
+        batch.step(frame_dt, substeps)
+        batch.get_state(host_np)
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e_start.elapsed_time(e_end)
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = vit_per_step * args.steps * world / (e2e_ms * 1e-3)
+    bytes_state = n_state * 4
+
+    # ---- roofline of the dominant kernel (the VBD colour kernel of the heaviest group)
+    groups = []
+    g = 0
+    while True:
+        el, mat, nl = C.c_int32(), C.c_int32(), C.c_int32()
+        fl, by = C.c_double(), C.c_double()
+        nv = C.c_int64()
+        if capi.lib().oct_batch_group_info(batch._h, g, C.byref(el), C.byref(mat), C.byref(fl), C.byref(by),
+                                           C.byref(nl), C.byref(nv)) != 0:
+            break
+        groups.append(dict(g=g, element=el.value, flops=fl.value, bytes=by.value, launches=nl.value,
+                           vertices=nv.value))
+        g += 1
+    dom = max(groups, key=lambda x: x["flops"])
+    sweeps = 10
+    ms = C.c_float()
+    capi.check(capi.lib().oct_batch_time_group(batch._h, dom["g"], 2, frame_dt / substeps, C.byref(ms)), "warm")
+    capi.check(capi.lib().oct_batch_time_group(batch._h, dom["g"], sweeps, frame_dt / substeps, C.byref(ms)),
+               "oct_batch_time_group")
+    per_launch_s = ms.value * 1e-3 / (sweeps * dom["launches"])
+    flops_per_launch = dom["flops"] / dom["launches"]
+    bytes_per_launch = dom["bytes"] / dom["launches"]
+    fp32_peak = C.c_double()
+    capi.lib().oct_fp32_peak(ctx.handle, C.byref(fp32_peak))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved_gbs = bytes_per_launch / per_launch_s / 1e9
+    achieved_tflops = flops_per_launch / per_launch_s / 1e12
+    traffic = None
+    try:
+        prof = json.load(open(os.path.join(ROOT, "profiles", "vbd_dram_traffic.json")))
+        traffic = prof.get("bytes_per_launch_scaled", {}).get(args.workload)
+    except Exception:
+        pass
+    roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                "frac": achieved_gbs / hbm_peak, "traffic": traffic,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
+                "kernel": "k_vertex<%d,3> (VBD colour sweep, element %d)" % (dom["element"], dom["element"]),
+                "binding_roof": "fp32",
+                "fp32": {"achieved_tflops": achieved_tflops, "peak_tflops": fp32_peak.value,
+                         "frac": achieved_tflops / fp32_peak.value,
+                         "peak_source": "oct_fp32_peak FMA loop, measured in this run"}}
+
+    # ---- plain single-scene drop-in path on the same scenes (FP32, per-colour launches)
+    plain = None
+    if not args.no_plain:
+        for s in scenes:
+            s.set_precision(ob.PREC_PLAIN)
+        for s in scenes:
+            s.step(frame_dt, substeps, sync=False)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for s in scenes:
+            s.step(frame_dt, substeps, sync=False)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = p0.elapsed_time(p1)
+        plain = {"value": vit_per_step / (plain_ms * 1e-3), "unit": "vertex-iter/s", "ms_per_step": plain_ms,
+                 "path": "each scene stepped alone through oct_scene_step: FP32, one launch per colour, no graph"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        every = 4 if args.workload == "batched" else 1
+        its = 4 if args.workload == "batched" else (2 if args.workload == "p2" else iterations)
+        v, secs, desc = cpu_reference(specs, iterations, substeps, frame_dt, threads, every, its)
+        cpu = {"value": v, "unit": "vertex-iter/s", "cores": threads, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": "vertex_iterations_per_s", "value": value, "unit": "vertex-iter/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "scenes": len(scenes), "free_nodes": free_nodes,
+                       "iterations": iterations, "substeps": substeps, "frame_dt": frame_dt,
+                       "precision": "mixed (FP32 bulk, compensated sums, FP64 ill-conditioned solves)",
+                       "seed": args.seed, "l2": "state larger than L2 (126 MB); no flush",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "p50_step_ms": float(np.percentile(step_ms, 50)), "p99_step_ms": float(np.percentile(step_ms, 99)),
+            "plain_dropin": plain,
+            "batched_over_plain": (value / world) / plain["value"] if plain else None,
+            "e2e": {"value": e2e_value, "unit": "vertex-iter/s", "h2d_bytes_per_step": bytes_state,
+                    "d2h_bytes_per_step": bytes_state},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+            "setup_s": setup_s,
+        }
+        print(json.dumps(line))
+    batch.close()
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,191 @@
+/* octopus_b200 — Blackwell (sm_100a) soft-body FEM time step, C ABI.
+ *
+ * Drop-in boundary for OctopusEngine's GPU solver objects.  One opaque scene bundles what
+ * the reference splits over several classes:
+ *   GPU_ParticleSystem(positions, masses)         octopus/include/GPU/GPU_ParticleSystem.h:54-73
+ *   GPU_VBD(ps, iteration, rho)                    octopus/include/GPU/VBD/GPU_VBD.h:15-26
+ *   GPU_VBD_FEM(element, topology, geometry, material, young, poisson, damping,
+ *               version, target_color)             octopus/include/GPU/VBD/GPU_VBD_FEM.h:62-65
+ *   GPU_PBD(global_damping) + GPU_PBD_FEM(...)     octopus/include/GPU/PBD/GPU_PBD.h:12-16,
+ *                                                  octopus/include/GPU/PBD/GPU_PBD_FEM.h:19-20
+ *   GPU_SemiExplicit + GPU_FEM_Explicit(...)       octopus/include/GPU/GPU_Integrator.h:34-36,
+ *                                                  octopus/include/GPU/Explicit/GPU_FEM_Explicit.h:14-15
+ *   GPU_Fix_Constraint(positions, Area*)           octopus/include/GPU/GPU_Constraint.h:11-18
+ *   Cuda_ParticleSystem_Dynamics::update (sub-step loop)
+ *                                                  octopus/src/Script/Dynamic/Cuda_ParticleSystem_Dynamic.cpp:17-31
+ * The C++ adapters in octopus_b200.hpp restore the reference class shapes on top of this.
+ *
+ * Conventions: every call returns an oct_status; arrays are plain host pointers unless a
+ * name says "device"; handles are owned by their context; one context per host thread.
+ */
+#ifndef OCTOPUS_B200_H
+#define OCTOPUS_B200_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum oct_status {
+    OCT_OK = 0,
+    OCT_EINVAL = 1,          /* bad argument */
+    OCT_ENOMEM_BUDGET = 2,   /* request exceeds the context's HBM budget (nothing allocated) */
+    OCT_ETIMEDOUT = 3,       /* a bounded device-side wait ran out */
+    OCT_ENUMERIC = 4,        /* NaN/Inf found in a scene's state */
+    OCT_ECUDA = 5,           /* a CUDA call failed; see oct_last_error */
+    OCT_ENOTSUP = 6          /* combination not supported */
+} oct_status;
+
+/* Element ids are the reference's Element enum values (octopus/include/Mesh/Elements.h:4-15). */
+enum { OCT_TETRA = 3, OCT_HEXA = 6, OCT_TETRA10 = 7, OCT_TETRA20 = 8, OCT_HEXA27 = 9 };
+/* Material enum (octopus/include/Dynamic/FEM/ContinuousMaterial.h:8-10). */
+enum { OCT_HOOKE = 0, OCT_STVK = 1, OCT_NEOHOOKE = 2, OCT_STABLE_NEOHOOKE = 3 };
+/* Mass_Distribution (octopus/include/Dynamic/FEM/FEM_Shape.h:693-696). */
+enum { OCT_MASS_UNIFORM = 0, OCT_MASS_FEMSHAPE = 1 };
+/* Solvers. */
+enum { OCT_SOLVER_VBD = 0, OCT_SOLVER_XPBD = 1, OCT_SOLVER_EXPLICIT = 2 };
+/* VBD_Version (octopus/include/GPU/VBD/GPU_VBD_FEM.h:13-15): Base, Threaded_Quadrature and
+ * Reduction_Symmetry update in place within a colour; Better_Coloration applies
+ * ColorReduction to target_color and updates all vertices of a colour from the same state. */
+enum { OCT_VBD_BASE = 0, OCT_VBD_THREADED_QUADRATURE = 1, OCT_VBD_REDUCTION_SYMMETRY = 2, OCT_VBD_BETTER_COLORATION = 3 };
+/* Colouring algorithms (octopus/include/Tools/Graph.h). */
+enum { OCT_COLOR_DSAT = 0, OCT_COLOR_GREEDY = 1 };
+/* Colour order per iteration: ascending (fixed, reproducible), or a std::shuffle with an
+ * std::mt19937 seeded once per scene (the reference reseeds from the clock each call). */
+enum { OCT_ORDER_ASCENDING = 0, OCT_ORDER_SHUFFLED = 1 };
+/* Precision: PLAIN = FP32 with the reference's Newton-skip rule (|det H| <= 1e-6);
+ * MIXED = FP32 bulk with compensated accumulation, FP64 Newton solve for ill-conditioned
+ * blocks, FP64 energy/residual reductions. */
+enum { OCT_PREC_PLAIN = 0, OCT_PREC_MIXED = 1 };
+
+typedef struct oct_ctx oct_ctx;
+typedef struct oct_scene oct_scene;
+typedef struct oct_batch oct_batch;
+typedef struct oct_server oct_server;
+
+typedef struct oct_scene_desc {
+    int32_t solver;                 /* OCT_SOLVER_* */
+    int32_t element;                /* OCT_TETRA ... OCT_HEXA27 */
+    int32_t n_nodes;
+    const float* positions;         /* n_nodes*3 rest positions (Mesh::Geometry) */
+    int32_t n_elements;
+    const int32_t* topology;        /* n_elements*nodes_per_element (Mesh::Topology) */
+    const float* masses;            /* n_nodes, or NULL: computed from density/mass_distribution */
+    float density;
+    int32_t mass_distribution;      /* OCT_MASS_* */
+    int32_t material;               /* OCT_HOOKE ... OCT_STABLE_NEOHOOKE */
+    float young, poisson;
+    const float* young_per_element; /* NULL or n_elements: per-element Young modulus */
+    float damping;                  /* VBD / explicit Rayleigh-like damping k_d */
+    float gravity[3];
+    int32_t n_fixed;                /* fixed-node list (GPU_Fix_Constraint ids)... */
+    const int32_t* fixed_ids;
+    int32_t fix_by_plane;           /* ...or nodes with dot(p - origin, normal) > 0 (Area::Plane) */
+    float plane_origin[3], plane_normal[3];
+    const float* initial_velocity;  /* NULL or n_nodes*3 */
+    /* VBD */
+    int32_t iterations;
+    float rho;                      /* Chebyshev spectral radius; 0 disables */
+    int32_t vbd_version;            /* OCT_VBD_* */
+    int32_t target_color;           /* for OCT_VBD_BETTER_COLORATION; < 0 means no reduction */
+    int32_t color_algo;             /* OCT_COLOR_* */
+    int32_t order_mode;             /* OCT_ORDER_* */
+    uint64_t seed;
+    /* XPBD */
+    float global_damping;
+    int32_t precision;              /* OCT_PREC_* */
+    int32_t box_limit;              /* 1: clamp free nodes to [box_min, box_max] each iteration */
+    float box_min[3], box_max[3];
+    int32_t threads_per_vertex;     /* 0 = autotune / default */
+} oct_scene_desc;
+
+/* Context: device, stream, HBM budget (bytes; 0 = 90% of free device memory). */
+oct_status oct_ctx_create(int device, size_t hbm_budget, oct_ctx** out);
+oct_status oct_ctx_destroy(oct_ctx* ctx);
+const char* oct_last_error(oct_ctx* ctx);
+oct_status oct_ctx_memory(oct_ctx* ctx, size_t* used, size_t* budget);
+void oct_desc_init(oct_scene_desc* d);   /* fills defaults (VBD, Stable NH, g = (0,-9.81,0)) */
+
+/* Scene = particle system + solver + FEM object + fix constraint.  Replaces
+ * Cuda_FEM_Dynamic::init (octopus/include/Script/Dynamic/Cuda_FEM_Dynamic.h:18-25). */
+oct_status oct_scene_create(oct_ctx* ctx, const oct_scene_desc* desc, oct_scene** out);
+oct_status oct_scene_destroy(oct_scene* s);
+/* Cuda_ParticleSystem_Dynamics::update: `substeps` integrator steps of frame_dt/substeps,
+ * asynchronous on the context stream (the reference's GPU_Integrator::step calls). */
+oct_status oct_scene_step(oct_scene* s, float frame_dt, int substeps);
+oct_status oct_scene_sync(oct_scene* s);
+/* GPU_ParticleSystem::get_position / get_velocity (synchronous D2H into host arrays). */
+oct_status oct_scene_get_positions(oct_scene* s, float* out_n3);
+oct_status oct_scene_get_velocities(oct_scene* s, float* out_n3);
+oct_status oct_scene_set_positions(oct_scene* s, const float* in_n3);
+oct_status oct_scene_set_velocities(oct_scene* s, const float* in_n3);
+oct_status oct_scene_info(oct_scene* s, int32_t* n_nodes, int32_t* n_elements, int32_t* n_colors, int32_t* n_fixed);
+/* Colouring and colour-sorted vertex order (GPU_VBD_FEM::create_buffers). */
+oct_status oct_scene_get_coloring(oct_scene* s, int32_t* colors, int32_t* vertex_order);
+/* Lumped masses used by the scene (compute_fem_mass). */
+oct_status oct_scene_get_masses(oct_scene* s, float* out_n);
+/* Move the fixed nodes rigidly: p = offset + com + R (init_p - com), R column-major 3x3
+ * (GPU_Fix_Constraint axis, octopus/src/GPU/GPU_Constraint.cu:108-112). */
+oct_status oct_scene_set_fixation(oct_scene* s, const float offset[3], const float rotation[9]);
+/* Switches the scene between OCT_PREC_PLAIN and OCT_PREC_MIXED for its own steps (a batch
+ * keeps the precision its scenes had when the batch was created). */
+oct_status oct_scene_set_precision(oct_scene* s, int precision);
+/* FP64 diagnostics: kinetic, elastic, gravity potential, total energy; and the VBD
+ * residual r = f - M/dt^2 (p - y) - damping term (kernel_vbd_compute_residual) as
+ * [sum |r|, max |r|] over free nodes.  Both return OCT_ENUMERIC on NaN/Inf state. */
+oct_status oct_scene_energy(oct_scene* s, double out4[4]);
+oct_status oct_scene_residual(oct_scene* s, float dt, double out2[2]);
+
+/* Batch: many VBD scenes stepped together, one launch per (element type, colour) across all
+ * scenes, driven by a per-scene work table, the sub-step captured as a CUDA graph.  All
+ * scenes must be VBD scenes of this context with equal iteration counts. */
+oct_status oct_batch_create(oct_ctx* ctx, oct_scene* const* scenes, int n, oct_batch** out);
+oct_status oct_batch_step(oct_batch* b, float frame_dt, int substeps);
+oct_status oct_batch_destroy(oct_batch* b);
+/* End-to-end helpers: upload all scenes' positions+velocities from one host array (scene
+ * order, n_i*6 floats each: p then v) and read them back. */
+oct_status oct_batch_set_state(oct_batch* b, const float* host_state);
+oct_status oct_batch_get_state(oct_batch* b, float* host_state);
+oct_status oct_batch_state_size(oct_batch* b, size_t* n_floats);
+
+/* Host-side scene building blocks (no GPU needed).
+ * Beam mesh as BeamMeshGenerator + promotions build it (octopus/src/Mesh/Generator/BeamGenerator.cpp:5-380):
+ * call with positions == NULL to get the sizes, then with arrays of those sizes. */
+oct_status oct_beam_mesh(int element, int nx, int ny, int nz, const float size[3], const float offset[3],
+                         int32_t* n_nodes, int32_t* n_elements, float* positions, int32_t* topology);
+/* compute_fem_mass (octopus/src/Dynamic/FEM/FEM_Shape.cpp:86-121). */
+oct_status oct_lumped_masses(int element, const float* positions, int n_nodes, const int32_t* topology, int n_elements,
+                             float density, int distribution, float* out_masses);
+/* Shape-function derivatives at the quadrature points (FEM_Shape::build): coords nq*3,
+ * weights nq, dN nq*nodes*3; any output may be NULL. */
+oct_status oct_shape_table(int element, int32_t* n_quadrature, double* coords, double* weights, double* dN);
+/* Vertex colouring as GPU_VBD_FEM::build_graph_color (DSAT or Greedy on the primal graph,
+ * optional ColorReduction to target when target > 0), or, with algo = 2, the element
+ * colouring of GPU_PBD_FEM::build_graph_color (Greedy_SLF on the vertex-dual graph; colors
+ * then has n_elements entries).  conflicts = same-colour adjacencies counted per multiset
+ * occurrence at both ends (GraphColoration::Get_Conflict summed). */
+oct_status oct_color(int element, const int32_t* topology, int n_elements, int n_nodes, int algo, int target,
+                     int32_t* colors, int32_t* n_colors, int64_t* conflicts);
+
+/* Measurement helpers.  The context's CUDA stream (cudaStream_t), to record events on it. */
+oct_status oct_ctx_stream(oct_ctx* ctx, void** stream);
+/* Measured FP32 FMA throughput of the device (TFLOP/s) from a register-resident FMA loop. */
+oct_status oct_fp32_peak(oct_ctx* ctx, double* tflops);
+/* Per element group g of a batch (scenes sharing element type, material and thread
+ * mapping): algorithmic FP32 flops and minimal DRAM bytes of one VBD colour sweep (all
+ * colours once), its launch count and vertex updates.  Returns OCT_EINVAL past the last group. */
+oct_status oct_batch_group_info(oct_batch* b, int g, int32_t* element, int32_t* material, double* flops_per_sweep,
+                                double* bytes_per_sweep, int32_t* launches_per_sweep, int64_t* vertices_per_sweep);
+/* Runs `sweeps` colour sweeps of group g alone on the context stream (outside the graph,
+ * state advances as in an iteration) and returns their total device time (CUDA events). */
+oct_status oct_batch_time_group(oct_batch* b, int g, int sweeps, float dt, float* ms);
+
+/* Device timing of the last oct_scene_step / oct_batch_step (ms, CUDA events). */
+oct_status oct_last_step_ms(oct_ctx* ctx, float* ms);
+/* Number of kernel launches issued by this context since creation. */
+oct_status oct_launch_count(oct_ctx* ctx, uint64_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,212 @@
+"""octopusengine_b200 — Blackwell-native soft-body FEM time step (VBD / XPBD / explicit).
+
+Python host-side handle on the C ABI (include/octopus_b200.h).  The classes mirror the
+reference's GPU solver objects and their host caller:
+
+    Context                 one device, one stream, one HBM budget
+    Scene                   GPU_ParticleSystem + GPU_VBD / GPU_PBD / GPU_SemiExplicit +
+                            GPU_VBD_FEM / GPU_PBD_FEM / GPU_FEM_Explicit + GPU_Fix_Constraint
+                            (octopus/include/Script/Dynamic/Cuda_FEM_Dynamic.h:18-25)
+    Scene.step(dt, n)       Cuda_ParticleSystem_Dynamics::update: n sub-steps of dt/n
+                            (octopus/src/Script/Dynamic/Cuda_ParticleSystem_Dynamic.cpp:17-31)
+    Scene.get_position()    GPU_ParticleSystem::get_position (octopus/include/GPU/GPU_ParticleSystem.h:54-61)
+    Batch                   many VBD scenes stepped by one launch per (element type, colour)
+
+Errors raise OctError with the library's status, as the C ABI returns it.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .capi import (COLOR_DSAT, COLOR_GREEDY, ELEMENT_NODES, HEXA, HEXA27, HOOKE, MASS_FEMSHAPE, MASS_UNIFORM,
+                   NEOHOOKE, ORDER_ASCENDING, ORDER_SHUFFLED, PREC_MIXED, PREC_PLAIN, SOLVER_EXPLICIT, SOLVER_VBD,
+                   SOLVER_XPBD, STABLE_NEOHOOKE, STVK, TETRA, TETRA10, TETRA20, VBD_BASE, VBD_BETTER_COLORATION,
+                   VBD_REDUCTION_SYMMETRY, OctError, beam_mesh, color, fixed_by_plane, lumped_masses, shape_table)
+
+__all__ = ["Context", "Scene", "Batch", "OctError", "beam_mesh", "color", "lumped_masses", "shape_table",
+           "fixed_by_plane", "library_path"]
+
+
+def library_path():
+    return capi.LIB_PATH
+
+
+class Context:
+    def __init__(self, device=0, hbm_budget=0):
+        self._h = C.c_void_p()
+        capi.check(capi.lib().oct_ctx_create(device, hbm_budget, C.byref(self._h)), "oct_ctx_create")
+        self._objs = []
+
+    @property
+    def handle(self):
+        return self._h
+
+    def memory(self):
+        used, budget = C.c_size_t(), C.c_size_t()
+        capi.check(capi.lib().oct_ctx_memory(self._h, C.byref(used), C.byref(budget)), "oct_ctx_memory")
+        return used.value, budget.value
+
+    def last_step_ms(self):
+        v = C.c_float()
+        capi.lib().oct_last_step_ms(self._h, C.byref(v))
+        return v.value
+
+    def launch_count(self):
+        v = C.c_uint64()
+        capi.lib().oct_launch_count(self._h, C.byref(v))
+        return v.value
+
+    def close(self):
+        if self._h:
+            for o in reversed(self._objs):
+                o.close()
+            self._objs = []
+            capi.lib().oct_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scene:
+    """One simulated object.  Keyword arguments map 1:1 onto oct_scene_desc fields."""
+
+    def __init__(self, ctx, element, positions, topology, **kw):
+        self.ctx = ctx
+        X = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        T = np.ascontiguousarray(topology, np.int32).reshape(-1, ELEMENT_NODES[element])
+        d = capi.SceneDesc()
+        capi.lib().oct_desc_init(C.byref(d))
+        keep = [X, T]
+        d.element = element
+        d.n_nodes = len(X)
+        d.positions = capi.ptr(X, C.c_float)
+        d.n_elements = len(T)
+        d.topology = capi.ptr(T, C.c_int32)
+        for k, v in kw.items():
+            if k in ("masses", "young_per_element", "initial_velocity"):
+                a = np.ascontiguousarray(v, np.float32).ravel()
+                keep.append(a)
+                setattr(d, k, capi.ptr(a, C.c_float))
+            elif k == "fixed_ids":
+                a = np.ascontiguousarray(v, np.int32).ravel()
+                keep.append(a)
+                d.fixed_ids = capi.ptr(a, C.c_int32) if len(a) else None
+                d.n_fixed = len(a)
+            elif k in ("gravity", "plane_origin", "plane_normal", "box_min", "box_max"):
+                setattr(d, k, (C.c_float * 3)(*v))
+            else:
+                setattr(d, k, v)
+        self._h = C.c_void_p()
+        capi.check(capi.lib().oct_scene_create(ctx.handle, C.byref(d), C.byref(self._h)), "oct_scene_create",
+                   ctx.handle)
+        ctx._objs.append(self)
+        nn, ne, nc, nf = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        capi.lib().oct_scene_info(self._h, C.byref(nn), C.byref(ne), C.byref(nc), C.byref(nf))
+        self.n_nodes, self.n_elements, self.n_colors, self.n_fixed = nn.value, ne.value, nc.value, nf.value
+        self.element = element
+        self.solver = kw.get("solver", SOLVER_VBD)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def step(self, frame_dt, substeps=1, sync=True):
+        capi.check(capi.lib().oct_scene_step(self._h, frame_dt, substeps), "oct_scene_step", self.ctx.handle)
+        if sync:
+            self.sync()
+
+    def sync(self):
+        capi.check(capi.lib().oct_scene_sync(self._h), "oct_scene_sync", self.ctx.handle)
+
+    def _get(self, fn):
+        out = np.zeros((self.n_nodes, 3), np.float32)
+        capi.check(fn(self._h, capi.ptr(out, C.c_float)), fn.__name__, self.ctx.handle)
+        return out
+
+    def get_position(self):
+        return self._get(capi.lib().oct_scene_get_positions)
+
+    def get_velocity(self):
+        return self._get(capi.lib().oct_scene_get_velocities)
+
+    def set_position(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        capi.check(capi.lib().oct_scene_set_positions(self._h, capi.ptr(p, C.c_float)), "oct_scene_set_positions")
+
+    def set_velocity(self, v):
+        v = np.ascontiguousarray(v, np.float32)
+        capi.check(capi.lib().oct_scene_set_velocities(self._h, capi.ptr(v, C.c_float)), "oct_scene_set_velocities")
+
+    def coloring(self):
+        c = np.zeros(self.n_nodes, np.int32)
+        o = np.zeros(self.n_nodes, np.int32)
+        capi.check(capi.lib().oct_scene_get_coloring(self._h, capi.ptr(c, C.c_int32), capi.ptr(o, C.c_int32)),
+                   "oct_scene_get_coloring")
+        return c, o
+
+    def masses(self):
+        m = np.zeros(self.n_nodes, np.float32)
+        capi.check(capi.lib().oct_scene_get_masses(self._h, capi.ptr(m, C.c_float)), "oct_scene_get_masses")
+        return m
+
+    def set_fixation(self, offset=(0, 0, 0), rotation=None):
+        off = np.asarray(offset, np.float32)
+        rot = np.eye(3, dtype=np.float32) if rotation is None else np.asarray(rotation, np.float32)
+        rot = np.ascontiguousarray(rot.T)   # column-major
+        capi.check(capi.lib().oct_scene_set_fixation(self._h, capi.ptr(off, C.c_float), capi.ptr(rot, C.c_float)),
+                   "oct_scene_set_fixation")
+
+    def set_precision(self, precision):
+        capi.check(capi.lib().oct_scene_set_precision(self._h, precision), "oct_scene_set_precision")
+
+    def energy(self):
+        e = np.zeros(4)
+        capi.check(capi.lib().oct_scene_energy(self._h, capi.ptr(e, C.c_double)), "oct_scene_energy",
+                   self.ctx.handle)
+        return e
+
+    def residual(self, dt):
+        r = np.zeros(2)
+        capi.check(capi.lib().oct_scene_residual(self._h, dt, capi.ptr(r, C.c_double)), "oct_scene_residual",
+                   self.ctx.handle)
+        return r
+
+    def close(self):
+        if self._h:
+            capi.lib().oct_scene_destroy(self._h)
+            self._h = C.c_void_p()
+
+
+class Batch:
+    """Many VBD scenes stepped together (one launch per element type and colour, CUDA graph)."""
+
+    def __init__(self, ctx, scenes):
+        self.ctx = ctx
+        self.scenes = list(scenes)
+        arr = (C.c_void_p * len(self.scenes))(*[s.handle.value for s in self.scenes])
+        self._h = C.c_void_p()
+        capi.check(capi.lib().oct_batch_create(ctx.handle, arr, len(self.scenes), C.byref(self._h)),
+                   "oct_batch_create", ctx.handle)
+        ctx._objs.append(self)
+        n = C.c_size_t()
+        capi.lib().oct_batch_state_size(self._h, C.byref(n))
+        self.state_size = n.value
+
+    def step(self, frame_dt, substeps=1):
+        capi.check(capi.lib().oct_batch_step(self._h, frame_dt, substeps), "oct_batch_step", self.ctx.handle)
+
+    def set_state(self, host):
+        capi.check(capi.lib().oct_batch_set_state(self._h, capi.ptr(host, C.c_float)), "oct_batch_set_state")
+
+    def get_state(self, host):
+        capi.check(capi.lib().oct_batch_get_state(self._h, capi.ptr(host, C.c_float)), "oct_batch_get_state")
+
+    def close(self):
+        if self._h:
+            capi.lib().oct_batch_destroy(self._h)
+            self._h = C.c_void_p()

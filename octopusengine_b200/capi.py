@@ -1,0 +1,185 @@
+"""ctypes binding of liboctb.so (the C ABI declared in include/octopus_b200.h).
+
+There is no fallback: if the library is missing or a CUDA device is absent, the calls
+raise.  The compute runs in the library's own CUDA kernels.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "liboctb.so")
+
+OK, EINVAL, ENOMEM_BUDGET, ETIMEDOUT, ENUMERIC, ECUDA, ENOTSUP = range(7)
+STATUS = {0: "OCT_OK", 1: "OCT_EINVAL", 2: "OCT_ENOMEM_BUDGET", 3: "OCT_ETIMEDOUT", 4: "OCT_ENUMERIC",
+          5: "OCT_ECUDA", 6: "OCT_ENOTSUP"}
+TETRA, HEXA, TETRA10, TETRA20, HEXA27 = 3, 6, 7, 8, 9
+ELEMENT_NODES = {TETRA: 4, HEXA: 8, TETRA10: 10, TETRA20: 20, HEXA27: 27}
+ELEMENT_QUADRATURE = {TETRA: 1, HEXA: 8, TETRA10: 4, TETRA20: 11, HEXA27: 27}
+HOOKE, STVK, NEOHOOKE, STABLE_NEOHOOKE = 0, 1, 2, 3
+MASS_UNIFORM, MASS_FEMSHAPE = 0, 1
+SOLVER_VBD, SOLVER_XPBD, SOLVER_EXPLICIT = 0, 1, 2
+VBD_BASE, VBD_THREADED_QUADRATURE, VBD_REDUCTION_SYMMETRY, VBD_BETTER_COLORATION = 0, 1, 2, 3
+COLOR_DSAT, COLOR_GREEDY = 0, 1
+ORDER_ASCENDING, ORDER_SHUFFLED = 0, 1
+PREC_PLAIN, PREC_MIXED = 0, 1
+
+EXPORTS = [
+    "oct_ctx_create", "oct_ctx_destroy", "oct_last_error", "oct_ctx_memory", "oct_desc_init",
+    "oct_scene_create", "oct_scene_destroy", "oct_scene_step", "oct_scene_sync", "oct_scene_get_positions",
+    "oct_scene_get_velocities", "oct_scene_set_positions", "oct_scene_set_velocities", "oct_scene_info",
+    "oct_scene_get_coloring", "oct_scene_get_masses", "oct_scene_set_fixation", "oct_scene_energy",
+    "oct_scene_residual", "oct_batch_create", "oct_batch_step", "oct_batch_destroy", "oct_batch_set_state",
+    "oct_batch_get_state", "oct_batch_state_size", "oct_beam_mesh", "oct_lumped_masses", "oct_shape_table",
+    "oct_color", "oct_last_step_ms", "oct_launch_count", "oct_ctx_stream", "oct_fp32_peak",
+    "oct_batch_group_info", "oct_batch_time_group", "oct_scene_set_precision",
+]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("solver", C.c_int32), ("element", C.c_int32), ("n_nodes", C.c_int32), ("positions", C.POINTER(C.c_float)),
+        ("n_elements", C.c_int32), ("topology", C.POINTER(C.c_int32)), ("masses", C.POINTER(C.c_float)),
+        ("density", C.c_float), ("mass_distribution", C.c_int32), ("material", C.c_int32),
+        ("young", C.c_float), ("poisson", C.c_float), ("young_per_element", C.POINTER(C.c_float)),
+        ("damping", C.c_float), ("gravity", C.c_float * 3), ("n_fixed", C.c_int32),
+        ("fixed_ids", C.POINTER(C.c_int32)), ("fix_by_plane", C.c_int32), ("plane_origin", C.c_float * 3),
+        ("plane_normal", C.c_float * 3), ("initial_velocity", C.POINTER(C.c_float)), ("iterations", C.c_int32),
+        ("rho", C.c_float), ("vbd_version", C.c_int32), ("target_color", C.c_int32), ("color_algo", C.c_int32),
+        ("order_mode", C.c_int32), ("seed", C.c_uint64), ("global_damping", C.c_float), ("precision", C.c_int32),
+        ("box_limit", C.c_int32), ("box_min", C.c_float * 3), ("box_max", C.c_float * 3),
+        ("threads_per_vertex", C.c_int32),
+    ]
+
+
+class OctError(RuntimeError):
+    def __init__(self, status, where, detail=""):
+        self.status = status
+        super().__init__("%s failed: %s %s" % (where, STATUS.get(status, status), detail))
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("liboctb.so is not built (run octopusengine_b200.build.build())")
+        L = C.CDLL(LIB_PATH)
+        vp, ip, fp, dp = C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_float), C.POINTER(C.c_double)
+        pp = C.POINTER(C.c_void_p)
+        sig = {
+            "oct_ctx_create": ([C.c_int, C.c_size_t, pp], C.c_int),
+            "oct_ctx_destroy": ([vp], C.c_int),
+            "oct_last_error": ([vp], C.c_char_p),
+            "oct_ctx_memory": ([vp, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)], C.c_int),
+            "oct_desc_init": ([C.POINTER(SceneDesc)], None),
+            "oct_scene_create": ([vp, C.POINTER(SceneDesc), pp], C.c_int),
+            "oct_scene_destroy": ([vp], C.c_int),
+            "oct_scene_step": ([vp, C.c_float, C.c_int], C.c_int),
+            "oct_scene_sync": ([vp], C.c_int),
+            "oct_scene_get_positions": ([vp, fp], C.c_int),
+            "oct_scene_get_velocities": ([vp, fp], C.c_int),
+            "oct_scene_set_positions": ([vp, fp], C.c_int),
+            "oct_scene_set_velocities": ([vp, fp], C.c_int),
+            "oct_scene_info": ([vp, ip, ip, ip, ip], C.c_int),
+            "oct_scene_get_coloring": ([vp, ip, ip], C.c_int),
+            "oct_scene_get_masses": ([vp, fp], C.c_int),
+            "oct_scene_set_fixation": ([vp, fp, fp], C.c_int),
+            "oct_scene_energy": ([vp, dp], C.c_int),
+            "oct_scene_residual": ([vp, C.c_float, dp], C.c_int),
+            "oct_batch_create": ([vp, pp, C.c_int, pp], C.c_int),
+            "oct_batch_step": ([vp, C.c_float, C.c_int], C.c_int),
+            "oct_batch_destroy": ([vp], C.c_int),
+            "oct_batch_set_state": ([vp, fp], C.c_int),
+            "oct_batch_get_state": ([vp, fp], C.c_int),
+            "oct_batch_state_size": ([vp, C.POINTER(C.c_size_t)], C.c_int),
+            "oct_beam_mesh": ([C.c_int, C.c_int, C.c_int, C.c_int, fp, fp, ip, ip, fp, ip], C.c_int),
+            "oct_lumped_masses": ([C.c_int, fp, C.c_int, ip, C.c_int, C.c_float, C.c_int, fp], C.c_int),
+            "oct_shape_table": ([C.c_int, ip, dp, dp, dp], C.c_int),
+            "oct_color": ([C.c_int, ip, C.c_int, C.c_int, C.c_int, C.c_int, ip, ip, C.POINTER(C.c_int64)], C.c_int),
+            "oct_last_step_ms": ([vp, fp], C.c_int),
+            "oct_launch_count": ([vp, C.POINTER(C.c_uint64)], C.c_int),
+            "oct_ctx_stream": ([vp, pp], C.c_int),
+            "oct_fp32_peak": ([vp, dp], C.c_int),
+            "oct_batch_group_info": ([vp, C.c_int, ip, ip, dp, dp, ip, C.POINTER(C.c_int64)], C.c_int),
+            "oct_batch_time_group": ([vp, C.c_int, C.c_int, C.c_float, fp], C.c_int),
+            "oct_scene_set_precision": ([vp, C.c_int], C.c_int),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def ptr(a, t):
+    return None if a is None else a.ctypes.data_as(C.POINTER(t))
+
+
+def check(status, where, ctx=None):
+    if status != OK:
+        detail = ""
+        if ctx is not None:
+            try:
+                detail = lib().oct_last_error(ctx).decode()
+            except Exception:
+                pass
+        raise OctError(status, where, detail)
+
+
+# ----------------------------------------------------------------------------- host helpers
+def beam_mesh(element, cells, size, offset=(0.0, 0.0, 0.0)):
+    L = lib()
+    nn, ne = C.c_int32(0), C.c_int32(0)
+    sz = np.asarray(size, np.float32)
+    off = np.asarray(offset, np.float32)
+    check(L.oct_beam_mesh(element, cells[0], cells[1], cells[2], ptr(sz, C.c_float), ptr(off, C.c_float),
+                          C.byref(nn), C.byref(ne), None, None), "oct_beam_mesh")
+    X = np.zeros((nn.value, 3), np.float32)
+    T = np.zeros((ne.value, ELEMENT_NODES[element]), np.int32)
+    check(L.oct_beam_mesh(element, cells[0], cells[1], cells[2], ptr(sz, C.c_float), ptr(off, C.c_float),
+                          C.byref(nn), C.byref(ne), ptr(X, C.c_float), ptr(T, C.c_int32)), "oct_beam_mesh")
+    return X, T
+
+
+def lumped_masses(element, X, T, density, distribution=MASS_FEMSHAPE):
+    X = np.ascontiguousarray(X, np.float32)
+    T = np.ascontiguousarray(T, np.int32)
+    m = np.zeros(len(X), np.float32)
+    check(lib().oct_lumped_masses(element, ptr(X, C.c_float), len(X), ptr(T, C.c_int32), len(T), density,
+                                  distribution, ptr(m, C.c_float)), "oct_lumped_masses")
+    return m
+
+
+def shape_table(element):
+    nq = ELEMENT_QUADRATURE[element]
+    ne = ELEMENT_NODES[element]
+    q = np.zeros(nq * 3)
+    w = np.zeros(nq)
+    d = np.zeros(nq * ne * 3)
+    n = C.c_int32(0)
+    check(lib().oct_shape_table(element, C.byref(n), ptr(q, C.c_double), ptr(w, C.c_double), ptr(d, C.c_double)),
+          "oct_shape_table")
+    return q.reshape(nq, 3), w, d.reshape(nq, ne, 3)
+
+
+def color(element, T, n_nodes, algo=COLOR_DSAT, target=-1):
+    T = np.ascontiguousarray(T, np.int32)
+    n = len(T) if algo == 2 else n_nodes
+    c = np.zeros(n, np.int32)
+    nc = C.c_int32(0)
+    conf = C.c_int64(0)
+    check(lib().oct_color(element, ptr(T, C.c_int32), len(T), n_nodes, algo, target, ptr(c, C.c_int32),
+                          C.byref(nc), C.byref(conf)), "oct_color")
+    return c, nc.value, conf.value
+
+
+def fixed_by_plane(X, origin, normal):
+    """Nodes with dot(p - origin, normal) > 0 in float32 (Area::Plane::inside)."""
+    X = np.asarray(X, np.float32)
+    d = ((X - np.float32(origin)) * np.float32(normal)).astype(np.float32)
+    return np.nonzero((d[:, 0] + d[:, 1]) + d[:, 2] > 0)[0].astype(np.int32)

@@ -1,0 +1,81 @@
+// Device-side data layout shared by the kernels and the host runtime.
+//
+// Node state is stored per scene as separate float4 arrays (structure of arrays, one
+// 16-byte vector per node so every gather is a single aligned load): the displacement
+// u = p - X (positions are X + u), the previous step's displacement, the inertial target
+// y with the lumped mass in .w, and the velocity.  Keeping u instead of p makes the
+// deformation gradient F = I + sum_i u_i (x) dNx_i free of the cancellation that absolute
+// positions cause in FP32 (F of the rest state is exactly I).
+//
+// Element data: topology E*NE ints, and per (element, quadrature point) a 48-byte record
+// of three float4: JX_inv (column-major 9 floats), V = |det J| w_q, lambda, mu.  The
+// inverse reference Jacobians are computed in FP64 on the host and rounded once.
+//
+// Colour-sorted vertex slots: vids[slot] is the node solved in that slot; slots of colour
+// c are [color_off[c], color_off[c+1]) in ascending node id (GPU_VBD_FEM::create_buffers,
+// octopus/src/GPU/VBD/GPU_VBD_FEM.cu:594-675); own_off/owners is the owner CSR in slot
+// order with owners packed as (element id << 5) | local node index.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace octb {
+
+constexpr int kMaxNE = 27;
+constexpr int kMaxNQ = 27;
+constexpr int kOwnerShift = 5;
+
+struct SceneDev {
+    float4* u;          // displacement, per node
+    float4* u_last;     // displacement at the start of the sub-step
+    float4* y;          // inertial target (xyz) and mass (w)
+    float4* v;          // velocity
+    float4* u_new;      // Jacobi scratch (colourings with conflicts)
+    float4* prev1;      // Chebyshev history (rho > 0)
+    float4* prev2;
+    int* mask;          // 1 = solved, 0 = fixed (GPU_ParticleSystem mask)
+    const float4* X;    // rest positions
+    const int* topo;    // n_elements * NE
+    const float4* eq;   // n_elements * NQ * 3
+    const int* vids;    // n_nodes, colour-sorted
+    const int* own_off; // n_nodes + 1, slot order
+    const int* owners;  // packed (eid << 5) | r
+    const int* fixed;   // n_fixed node ids
+    int n_nodes, n_elements, n_fixed, element;
+    float damping;      // k_d
+    float gx, gy, gz;
+    float comx, comy, comz;            // fixed-set centre of mass (float, as the reference)
+    float offx, offy, offz;            // fixation offset
+    float rot[9];                      // fixation rotation, column-major
+    float bminx, bminy, bminz, bmaxx, bmaxy, bmaxz;
+    int box_limit;
+    int precision;                     // 0 plain, 1 mixed
+};
+
+// One block-sized unit of colour work: `count` consecutive colour slots of one scene.
+struct VWork {
+    int scene;
+    int slot_begin;
+    int count;
+    int pad;
+};
+
+// One unit of node-parallel work (predictor, velocity update, Chebyshev).
+struct NWork {
+    int scene;
+    int begin;
+    int count;
+    int pad;
+};
+
+struct StepParams {
+    float dt;
+    float inv_dt;
+    float omega;         // Chebyshev weight of this iteration
+    int iteration;       // iteration index within the sub-step
+    const int* pending_v0;   // per scene: 1 until its first sub-step has consumed the initial velocity
+    int in_place;        // 1: write u directly, 0: write u_new (Jacobi within a colour)
+    int* error;          // device error word (bounded waits, non-finite results)
+};
+
+}  // namespace octb

@@ -1,0 +1,32 @@
+// Host-callable launchers of the kernels in kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace octb {
+
+cudaError_t upload_shape_tables(int element, const float* dN, int n_floats);
+// mode 0: VBD solve, 1: VBD residual (red[0] += |r|, red[1] = max |r|), 2: explicit force
+void launch_vertex(int element, int material, const SceneDev* scenes, const VWork* work, int n_work, int tpv, int mode,
+                   const StepParams& P, double* red, cudaStream_t st);
+void launch_commit(const SceneDev* scenes, const VWork* work, int n_work, cudaStream_t st);
+// kind 0: VBD predictor, kind 1: semi-implicit Euler (use_force: add the force in u_new)
+void launch_predict(const SceneDev* scenes, const NWork* work, int n_work, int kind, int use_force, int chebyshev,
+                    const StepParams& P, cudaStream_t st);
+void launch_velocity(const SceneDev* scenes, const NWork* work, int n_work, float global_damping, int pbd,
+                     const StepParams& P, cudaStream_t st);
+void launch_chebyshev(const SceneDev* scenes, const NWork* work, int n_work, const StepParams& P, cudaStream_t st);
+// box_pass 0: work indexes fixed-id chunks; 1: work indexes node chunks (box clamp)
+void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, int box_pass, cudaStream_t st);
+void launch_xpbd(int element, int material, const SceneDev* scenes, const int* elems, int begin, int count, int scene,
+                 const StepParams& P, cudaStream_t st);
+void launch_energy(int element, int material, const SceneDev* scenes, int scene, int n_nodes, int n_elements, double* out,
+                   int* error, cudaStream_t st);
+
+// FP32 FMA microbenchmark: returns the number of FMAs issued by the launch.
+double launch_fma_peak(cudaStream_t st);
+// Algorithmic FP32 flops of one (owner, quadrature point) term of the VBD kernel.
+double vbd_term_flops(int element, int material);
+
+}  // namespace octb

@@ -1,0 +1,977 @@
+// Host runtime behind the C ABI: contexts (device, stream, HBM budget), scenes (set-up on
+// the host, state resident on the device), the per-scene step drivers that follow the
+// reference's launch structure, and batches that step many scenes through one launch per
+// (element type, colour) captured in a CUDA graph.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/octopus_b200.h"
+#include "device.cuh"
+#include "host.hpp"
+#include "kernels.cuh"
+
+using namespace octb;
+
+namespace {
+constexpr int kBlockThreads = 128;
+constexpr int kNodeChunk = 256;
+}  // namespace
+
+struct oct_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    size_t budget = 0, used = 0;
+    std::string err;
+    int* d_error = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.f;
+    uint64_t launches = 0;
+    bool tables[10] = {false};
+    std::mutex mu;   // guards the budget accounting and the shape-table upload
+};
+
+namespace {
+
+oct_status fail(oct_ctx* c, oct_status s, const std::string& msg) {
+    if (c) c->err = msg;
+    return s;
+}
+
+#define OCT_CUDA(ctx, call)                                                                        \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return fail(ctx, OCT_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+// Device allocation accounted against the context budget.
+struct DevMem {
+    oct_ctx* ctx = nullptr;
+    std::vector<std::pair<void*, size_t>> blocks;
+    template <class T> oct_status alloc(T*& p, size_t n) {
+        const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        if (ctx->used + bytes > ctx->budget)
+            return fail(ctx, OCT_ENOMEM_BUDGET, "HBM budget exceeded: need " + std::to_string(ctx->used + bytes) +
+                                                    " bytes, budget " + std::to_string(ctx->budget));
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, bytes);
+        if (e != cudaSuccess) return fail(ctx, OCT_ECUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        blocks.push_back({q, bytes});
+        ctx->used += bytes;
+        p = (T*)q;
+        return OCT_OK;
+    }
+    void release() {
+        std::lock_guard<std::mutex> lock(ctx->mu);
+        for (auto& b : blocks) { cudaFree(b.first); ctx->used -= b.second; }
+        blocks.clear();
+    }
+};
+
+}  // namespace
+
+struct oct_scene {
+    oct_ctx* ctx = nullptr;
+    DevMem mem;
+    int solver = 0, element = 0, material = 0, ne = 0, nq = 0;
+    int n_nodes = 0, n_elements = 0, n_fixed = 0, n_colors = 0;
+    int iterations = 1, order_mode = 0, tpv = 8, precision = 0;
+    float rho = 0.f, global_damping = 0.f;
+    bool in_place = true, box = false, has_v0 = false;
+    std::mt19937 rng;
+    std::vector<int32_t> colors, vids, color_off;   // colour-sorted slots
+    std::vector<float> masses, X;
+    std::vector<int32_t> fixed;
+    // device
+    SceneDev h{};
+    SceneDev* d_scene = nullptr;
+    int* d_pending = nullptr;
+    int pending_host = 0;
+    VWork* d_vwork = nullptr;
+    std::vector<int> vwork_off;     // per colour: [vwork_off[c], vwork_off[c+1])
+    NWork* d_nwork = nullptr;
+    int n_nwork = 0;
+    NWork* d_fwork = nullptr;
+    int n_fwork = 0;
+    int* d_elems = nullptr;         // XPBD: colour-sorted element ids
+    std::vector<int> elem_off;
+    double* d_red = nullptr;        // 4 doubles of reduction scratch
+};
+
+struct oct_batch {
+    oct_ctx* ctx = nullptr;
+    DevMem mem;
+    std::vector<oct_scene*> scenes;
+    SceneDev* d_scenes = nullptr;
+    int* d_pending = nullptr;
+    std::vector<int> pending_host;
+    struct Group {
+        int element, material, tpv;
+        bool in_place;
+        std::vector<int> off;   // per colour, into the group's part of d_vwork
+        int base = 0;
+        cudaStream_t stream = nullptr;
+        cudaEvent_t done = nullptr;
+    };
+    std::vector<Group> groups;
+    VWork* d_vwork = nullptr;
+    NWork* d_nwork = nullptr;
+    int n_nwork = 0;
+    NWork* d_fwork = nullptr;
+    int n_fwork = 0;
+    NWork* d_bwork = nullptr;
+    int n_bwork = 0;
+    int iterations = 1;
+    float rho = 0.f;
+    cudaEvent_t fork = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    float graph_dt = -1.f;
+    int graph_pending = -1;
+    std::vector<size_t> state_off;
+};
+
+namespace {
+
+oct_status ensure_tables(oct_ctx* c, int element) {
+    std::lock_guard<std::mutex> lock(c->mu);
+    if (c->tables[element]) return OCT_OK;
+    ShapeTable s;
+    if (!shape_table(element, s)) return fail(c, OCT_EINVAL, "unsupported element");
+    std::vector<float> f(s.dN.begin(), s.dN.end());
+    f.resize(((f.size() + 3) / 4) * 4, 0.f);
+    OCT_CUDA(c, upload_shape_tables(element, f.data(), (int)s.dN.size()));
+    c->tables[element] = true;
+    return OCT_OK;
+}
+
+// Split [begin, end) slots into block-sized work items for one scene.
+void append_vwork(std::vector<VWork>& out, int scene, int begin, int end, int tpv) {
+    const int vpb = kBlockThreads / tpv;
+    for (int s = begin; s < end; s += vpb) out.push_back({scene, s, std::min(vpb, end - s), 0});
+}
+void append_nwork(std::vector<NWork>& out, int scene, int n) {
+    for (int s = 0; s < n; s += kNodeChunk) out.push_back({scene, s, std::min(kNodeChunk, n - s), 0});
+}
+
+int default_tpv(int element) {
+    switch (element) {
+        case kTetra: return 8;
+        case kHexa: return 8;
+        case kTetra10: return 8;
+        case kTetra20: return 8;
+        default: return 4;
+    }
+}
+
+template <class T> oct_status upload(oct_ctx* c, DevMem& m, T*& d, const std::vector<T>& h) {
+    oct_status st = m.alloc(d, h.size());
+    if (st) return st;
+    if (!h.empty()) OCT_CUDA(c, cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return OCT_OK;
+}
+
+oct_status check_error_word(oct_ctx* c) {
+    int e = 0;
+    OCT_CUDA(c, cudaMemcpy(&e, c->d_error, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e & 2) { int z = 0; cudaMemcpy(c->d_error, &z, sizeof(int), cudaMemcpyHostToDevice); return fail(c, OCT_ENUMERIC, "non-finite value in the scene state"); }
+    if (e & 1) { int z = 0; cudaMemcpy(c->d_error, &z, sizeof(int), cudaMemcpyHostToDevice); return fail(c, OCT_ETIMEDOUT, "a bounded device wait timed out"); }
+    return OCT_OK;
+}
+
+oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
+    s->ctx = c;
+    s->mem.ctx = c;
+    s->solver = d->solver;
+    s->element = d->element;
+    s->material = d->material;
+    s->ne = element_nodes(d->element);
+    s->nq = element_quadrature(d->element);
+    if (s->ne < 0) return fail(c, OCT_EINVAL, "unsupported element type");
+    if (d->material < 0 || d->material > 3) return fail(c, OCT_EINVAL, "unsupported material");
+    if (d->n_nodes <= 0 || d->n_elements <= 0 || !d->positions || !d->topology) return fail(c, OCT_EINVAL, "empty mesh");
+    if (d->solver < 0 || d->solver > 2) return fail(c, OCT_EINVAL, "unknown solver");
+    s->n_nodes = d->n_nodes;
+    s->n_elements = d->n_elements;
+    const int N = s->n_nodes, E = s->n_elements, NE = s->ne, NQ = s->nq;
+    for (int64_t k = 0; k < (int64_t)E * NE; ++k)
+        if (d->topology[k] < 0 || d->topology[k] >= N) return fail(c, OCT_EINVAL, "topology index out of range");
+    if ((int64_t)E >= (1ll << (31 - kOwnerShift))) return fail(c, OCT_EINVAL, "too many elements for one scene");
+    oct_status st = ensure_tables(c, d->element);
+    if (st) return st;
+    s->iterations = std::max(1, d->iterations);
+    s->rho = d->rho;
+    s->order_mode = d->order_mode;
+    s->rng.seed((unsigned)d->seed);
+    s->precision = d->precision;
+    s->global_damping = d->global_damping;
+    s->box = d->box_limit != 0;
+    s->has_v0 = d->initial_velocity != nullptr;
+    s->tpv = d->threads_per_vertex > 0 ? d->threads_per_vertex : default_tpv(d->element);
+    if (s->tpv != 1 && s->tpv != 2 && s->tpv != 4 && s->tpv != 8 && s->tpv != 16 && s->tpv != 32)
+        return fail(c, OCT_EINVAL, "threads_per_vertex must be a power of two <= 32");
+    s->X.assign(d->positions, d->positions + 3 * (size_t)N);
+
+    // masses (Cuda_FEM_Dynamic::get_fem_masses)
+    if (d->masses) s->masses.assign(d->masses, d->masses + N);
+    else lumped_masses(d->element, d->positions, N, d->topology, E, d->density, d->mass_distribution, s->masses);
+    for (int i = 0; i < N; ++i)
+        if (!(s->masses[i] > 0.f)) return fail(c, OCT_EINVAL, "non-positive node mass (node not in any element?)");
+
+    // fixed nodes: explicit ids or Area::Plane test, ascending (GPU_Fix_Constraint ctor)
+    if (d->fix_by_plane) {
+        for (int i = 0; i < N; ++i) {
+            const float* p = d->positions + 3 * i;
+            const float v = (p[0] - d->plane_origin[0]) * d->plane_normal[0] + (p[1] - d->plane_origin[1]) * d->plane_normal[1] +
+                            (p[2] - d->plane_origin[2]) * d->plane_normal[2];
+            if (v > 0.f) s->fixed.push_back(i);
+        }
+    } else if (d->n_fixed > 0 && d->fixed_ids) {
+        s->fixed.assign(d->fixed_ids, d->fixed_ids + d->n_fixed);
+        for (int id : s->fixed) if (id < 0 || id >= N) return fail(c, OCT_EINVAL, "fixed id out of range");
+    }
+    s->n_fixed = (int)s->fixed.size();
+    float cx = 0, cy = 0, cz = 0;
+    for (int id : s->fixed) { cx += d->positions[3 * id]; cy += d->positions[3 * id + 1]; cz += d->positions[3 * id + 2]; }
+    if (s->n_fixed) { cx /= (float)s->n_fixed; cy /= (float)s->n_fixed; cz /= (float)s->n_fixed; }
+
+    // precompute per (element, quadrature point) in FP64 (GPU_FEM::build_fem_const,
+    // octopus/src/GPU/GPU_FEM.cu:176-215) with the Lame parameters of GPU_FEM.cu:162-163
+    ShapeTable sh;
+    shape_table(d->element, sh);
+    std::vector<float4> eq((size_t)E * NQ * 3);
+    for (int e = 0; e < E; ++e) {
+        const double Y = d->young_per_element ? d->young_per_element[e] : d->young, nu = d->poisson;
+        const float lam = (float)(Y * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))), mu = (float)(Y / (2.0 * (1.0 + nu)));
+        for (int q = 0; q < NQ; ++q) {
+            double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};   // J[col][row] = sum_k X_k[row] dN_qk[col]
+            for (int k = 0; k < NE; ++k) {
+                const float* x = d->positions + 3 * d->topology[(size_t)e * NE + k];
+                const double* dn = &sh.dN[((size_t)q * NE + k) * 3];
+                for (int cc = 0; cc < 3; ++cc) for (int r = 0; r < 3; ++r) J[cc][r] += (double)x[r] * dn[cc];
+            }
+            const double det = J[0][0] * (J[1][1] * J[2][2] - J[2][1] * J[1][2]) - J[1][0] * (J[0][1] * J[2][2] - J[2][1] * J[0][2]) +
+                               J[2][0] * (J[0][1] * J[1][2] - J[1][1] * J[0][2]);
+            if (!(std::fabs(det) > 0.0)) return fail(c, OCT_EINVAL, "degenerate element " + std::to_string(e));
+            const double id = 1.0 / det;
+            double I[3][3];   // inverse, I[col][row]
+            I[0][0] = (J[1][1] * J[2][2] - J[2][1] * J[1][2]) * id;
+            I[1][0] = -(J[1][0] * J[2][2] - J[2][0] * J[1][2]) * id;
+            I[2][0] = (J[1][0] * J[2][1] - J[2][0] * J[1][1]) * id;
+            I[0][1] = -(J[0][1] * J[2][2] - J[2][1] * J[0][2]) * id;
+            I[1][1] = (J[0][0] * J[2][2] - J[2][0] * J[0][2]) * id;
+            I[2][1] = -(J[0][0] * J[2][1] - J[2][0] * J[0][1]) * id;
+            I[0][2] = (J[0][1] * J[1][2] - J[1][1] * J[0][2]) * id;
+            I[1][2] = -(J[0][0] * J[1][2] - J[1][0] * J[0][2]) * id;
+            I[2][2] = (J[0][0] * J[1][1] - J[1][0] * J[0][1]) * id;
+            const float V = (float)(std::fabs(det) * sh.w[q]);
+            float4* r = &eq[((size_t)e * NQ + q) * 3];
+            r[0] = make_float4((float)I[0][0], (float)I[0][1], (float)I[0][2], (float)I[1][0]);
+            r[1] = make_float4((float)I[1][1], (float)I[1][2], (float)I[2][0], (float)I[2][1]);
+            r[2] = make_float4((float)I[2][2], V, lam, mu);
+        }
+    }
+
+    // colouring and slot order
+    std::vector<int32_t> slot_vids;
+    std::vector<std::vector<int32_t>> elems_by_color;
+    if (d->solver == OCT_SOLVER_VBD) {
+        PrimalGraph g;
+        build_primal_graph(NE, d->topology, E, N, g);
+        Coloring col = d->color_algo == OCT_COLOR_GREEDY ? color_greedy(g) : color_dsat(g);
+        if (d->vbd_version == OCT_VBD_BETTER_COLORATION && d->target_color > 0 && d->target_color < col.n_colors)
+            color_reduction(g, col, d->target_color);
+        s->in_place = count_conflicts(g, col) == 0;
+        s->colors = col.colors;
+        s->n_colors = col.n_colors;
+    } else if (d->solver == OCT_SOLVER_XPBD) {
+        PrimalGraph g;
+        build_dual_vertex_graph(NE, d->topology, E, N, g);
+        Coloring col = color_greedy_slf(g);
+        s->n_colors = col.n_colors;
+        s->colors.assign(N, 0);
+        elems_by_color.assign(col.n_colors, {});
+        for (int e = 0; e < E; ++e) elems_by_color[col.colors[e]].push_back(e);   // build_thread_by_color
+    } else {
+        s->n_colors = 1;
+        s->colors.assign(N, 0);
+    }
+    if (d->solver == OCT_SOLVER_XPBD) {
+        s->n_colors = (int)elems_by_color.size();
+        s->elem_off.assign(1, 0);
+        std::vector<int32_t> flat;
+        for (auto& v : elems_by_color) { flat.insert(flat.end(), v.begin(), v.end()); s->elem_off.push_back((int)flat.size()); }
+        if ((st = upload(c, s->mem, s->d_elems, flat))) return st;
+        // VBD-style slots are unused; keep the identity order for the getters
+        for (int i = 0; i < N; ++i) slot_vids.push_back(i);
+        s->color_off = {0, N};
+    } else {
+        const int C = s->n_colors;
+        s->color_off.assign(C + 1, 0);
+        for (int i = 0; i < N; ++i) s->color_off[s->colors[i] + 1]++;
+        for (int k = 0; k < C; ++k) s->color_off[k + 1] += s->color_off[k];
+        slot_vids.resize(N);
+        std::vector<int> fillp(s->color_off.begin(), s->color_off.end() - 1);
+        for (int i = 0; i < N; ++i) slot_vids[fillp[s->colors[i]]++] = i;   // ascending id within colour
+    }
+    s->vids = slot_vids;
+
+    // owner CSR in slot order (build_owner_data, GPU_VBD_FEM.cu:677-690: element order)
+    std::vector<int32_t> cnt(N, 0);
+    for (int64_t k = 0; k < (int64_t)E * NE; ++k) cnt[d->topology[k]]++;
+    std::vector<int64_t> voff(N + 1, 0);
+    for (int i = 0; i < N; ++i) voff[i + 1] = voff[i] + cnt[i];
+    std::vector<int32_t> vown(voff[N]);
+    std::vector<int64_t> vf(voff.begin(), voff.end() - 1);
+    for (int e = 0; e < E; ++e)
+        for (int j = 0; j < NE; ++j) vown[vf[d->topology[(size_t)e * NE + j]]++] = (e << kOwnerShift) | j;
+    std::vector<int32_t> own_off(N + 1, 0), owners;
+    owners.reserve(vown.size());
+    for (int sl = 0; sl < N; ++sl) {
+        const int v = slot_vids[sl];
+        owners.insert(owners.end(), vown.begin() + voff[v], vown.begin() + voff[v + 1]);
+        own_off[sl + 1] = (int32_t)owners.size();
+    }
+
+    // device state
+    std::vector<float4> X4(N), y4(N), zero4(N, make_float4(0, 0, 0, 0)), v4(N, make_float4(0, 0, 0, 0));
+    for (int i = 0; i < N; ++i) {
+        X4[i] = make_float4(d->positions[3 * i], d->positions[3 * i + 1], d->positions[3 * i + 2], 0.f);
+        y4[i] = make_float4(0.f, 0.f, 0.f, s->masses[i]);
+        if (d->initial_velocity)
+            v4[i] = make_float4(d->initial_velocity[3 * i], d->initial_velocity[3 * i + 1], d->initial_velocity[3 * i + 2], 0.f);
+    }
+    std::vector<int32_t> mask(N, 1);
+    std::vector<int32_t> topo(d->topology, d->topology + (size_t)E * NE);
+    SceneDev& h = s->h;
+    float4 *u, *ul, *y, *v, *un, *p1 = nullptr, *p2 = nullptr, *Xd;
+    if ((st = upload(c, s->mem, u, zero4)) || (st = upload(c, s->mem, ul, zero4)) || (st = upload(c, s->mem, y, y4)) ||
+        (st = upload(c, s->mem, v, v4)) || (st = upload(c, s->mem, Xd, X4)))
+        return st;
+    if ((st = s->mem.alloc(un, N))) return st;
+    OCT_CUDA(c, cudaMemset(un, 0, sizeof(float4) * N));
+    if (s->rho > 0.f) {
+        if ((st = upload(c, s->mem, p1, zero4)) || (st = upload(c, s->mem, p2, zero4))) return st;
+    }
+    int *maskd, *topod, *vidsd, *offd, *ownd, *fixd = nullptr;
+    float4* eqd;
+    if ((st = upload(c, s->mem, maskd, mask)) || (st = upload(c, s->mem, topod, topo)) || (st = upload(c, s->mem, eqd, eq)) ||
+        (st = upload(c, s->mem, vidsd, slot_vids)) || (st = upload(c, s->mem, offd, own_off)) || (st = upload(c, s->mem, ownd, owners)))
+        return st;
+    if (s->n_fixed && (st = upload(c, s->mem, fixd, s->fixed))) return st;
+    h.u = u; h.u_last = ul; h.y = y; h.v = v; h.u_new = un; h.prev1 = p1; h.prev2 = p2; h.mask = maskd; h.X = Xd;
+    h.topo = topod; h.eq = eqd; h.vids = vidsd; h.own_off = offd; h.owners = ownd; h.fixed = fixd;
+    h.n_nodes = N; h.n_elements = E; h.n_fixed = s->n_fixed; h.element = d->element;
+    h.damping = d->damping;
+    h.gx = d->gravity[0]; h.gy = d->gravity[1]; h.gz = d->gravity[2];
+    h.comx = cx; h.comy = cy; h.comz = cz;
+    h.offx = h.offy = h.offz = 0.f;
+    for (int k = 0; k < 9; ++k) h.rot[k] = (k % 4 == 0) ? 1.f : 0.f;
+    h.bminx = d->box_min[0]; h.bminy = d->box_min[1]; h.bminz = d->box_min[2];
+    h.bmaxx = d->box_max[0]; h.bmaxy = d->box_max[1]; h.bmaxz = d->box_max[2];
+    h.box_limit = s->box;
+    h.precision = s->precision;
+    if ((st = s->mem.alloc(s->d_scene, 1))) return st;
+    OCT_CUDA(c, cudaMemcpy(s->d_scene, &h, sizeof(SceneDev), cudaMemcpyHostToDevice));
+    s->pending_host = s->has_v0 ? 1 : 0;
+    if ((st = upload(c, s->mem, s->d_pending, std::vector<int>{s->pending_host}))) return st;
+    if ((st = s->mem.alloc(s->d_red, 4))) return st;
+
+    // work tables
+    std::vector<VWork> vw;
+    s->vwork_off.assign(1, 0);
+    for (int k = 0; k + 1 < (int)s->color_off.size(); ++k) {
+        append_vwork(vw, 0, s->color_off[k], s->color_off[k + 1], s->tpv);
+        s->vwork_off.push_back((int)vw.size());
+    }
+    std::vector<NWork> nw, fw;
+    append_nwork(nw, 0, N);
+    append_nwork(fw, 0, s->n_fixed);
+    s->n_nwork = (int)nw.size();
+    s->n_fwork = (int)fw.size();
+    if ((st = upload(c, s->mem, s->d_vwork, vw)) || (st = upload(c, s->mem, s->d_nwork, nw)) || (st = upload(c, s->mem, s->d_fwork, fw)))
+        return st;
+    return OCT_OK;
+}
+
+StepParams base_params(oct_ctx* c, float dt) {
+    StepParams P{};
+    P.dt = dt;
+    P.inv_dt = 1.f / dt;
+    P.omega = 1.f;
+    P.error = c->d_error;
+    return P;
+}
+
+// One GPU_VBD::step (octopus/src/GPU/VBD/GPU_VBD.cu:38-61) of one scene with the reference's
+// launch structure: predictor, iterations x (one launch per colour [+ commit] + constraints
+// [+ Chebyshev]), velocity update.
+void vbd_substep(oct_scene* s, float dt) {
+    oct_ctx* c = s->ctx;
+    cudaStream_t st = c->stream;
+    StepParams P = base_params(c, dt);
+    P.pending_v0 = s->d_pending;
+    P.in_place = s->in_place ? 1 : 0;
+    const bool cheb = s->rho > 0.f && s->rho > 1.17549435e-38f * 1e6f;
+    launch_predict(s->d_scene, s->d_nwork, s->n_nwork, 0, 0, cheb ? 1 : 0, P, st);
+    c->launches++;
+    if (s->pending_host) {
+        cudaMemsetAsync(s->d_pending, 0, sizeof(int), st);
+        s->pending_host = 0;
+    }
+    std::vector<int> order(s->n_colors);
+    float omega = 1.f;
+    for (int j = 0; j < s->iterations; ++j) {
+        std::iota(order.begin(), order.end(), 0);
+        if (s->order_mode == OCT_ORDER_SHUFFLED) std::shuffle(order.begin(), order.end(), s->rng);
+        for (int k : order) {
+            const int b = s->vwork_off[k], n = s->vwork_off[k + 1] - b;
+            launch_vertex(s->element, s->material, s->d_scene, s->d_vwork + b, n, s->tpv, 0, P, nullptr, st);
+            c->launches++;
+            if (!s->in_place) { launch_commit(s->d_scene, s->d_vwork + b, n, st); c->launches++; }
+        }
+        if (s->n_fixed) { launch_constraints(s->d_scene, s->d_fwork, s->n_fwork, 0, st); c->launches++; }
+        if (s->box) { launch_constraints(s->d_scene, s->d_nwork, s->n_nwork, 1, st); c->launches++; }
+        if (cheb) {
+            if (j == 1) omega = 2.f / (2.f - s->rho * s->rho);
+            else if (j > 1) omega = 4.f / (4.f - s->rho * s->rho * omega);
+            P.omega = omega;
+            P.iteration = j;
+            launch_chebyshev(s->d_scene, s->d_nwork, s->n_nwork, P, st);
+            c->launches++;
+        }
+    }
+    launch_velocity(s->d_scene, s->d_nwork, s->n_nwork, 0.f, 0, P, st);
+    c->launches++;
+}
+
+// GPU_PBD::step (octopus/src/GPU/PBD/GPU_PBD.cu:20-26).
+void xpbd_substep(oct_scene* s, float dt) {
+    oct_ctx* c = s->ctx;
+    cudaStream_t st = c->stream;
+    StepParams P = base_params(c, dt);
+    launch_predict(s->d_scene, s->d_nwork, s->n_nwork, 1, 0, 0, P, st);
+    c->launches++;
+    for (int k = 0; k < s->n_colors; ++k) {
+        launch_xpbd(s->element, s->material, s->d_scene, s->d_elems, s->elem_off[k], s->elem_off[k + 1] - s->elem_off[k], 0, P, st);
+        c->launches++;
+    }
+    if (s->n_fixed) { launch_constraints(s->d_scene, s->d_fwork, s->n_fwork, 0, st); c->launches++; }
+    if (s->box) { launch_constraints(s->d_scene, s->d_nwork, s->n_nwork, 1, st); c->launches++; }
+    launch_velocity(s->d_scene, s->d_nwork, s->n_nwork, s->global_damping, 1, P, st);
+    c->launches++;
+}
+
+// GPU_SemiExplicit::step (octopus/src/GPU/GPU_Integrator.cu:36-42).
+void explicit_substep(oct_scene* s, float dt) {
+    oct_ctx* c = s->ctx;
+    cudaStream_t st = c->stream;
+    StepParams P = base_params(c, dt);
+    launch_vertex(s->element, s->material, s->d_scene, s->d_vwork, s->vwork_off[1], s->tpv, 2, P, nullptr, st);
+    launch_predict(s->d_scene, s->d_nwork, s->n_nwork, 1, 1, 0, P, st);
+    c->launches += 2;
+    if (s->n_fixed) { launch_constraints(s->d_scene, s->d_fwork, s->n_fwork, 0, st); c->launches++; }
+    if (s->box) { launch_constraints(s->d_scene, s->d_nwork, s->n_nwork, 1, st); c->launches++; }
+}
+
+oct_status read_nodes(oct_scene* s, const float4* d, float* out, bool add_rest) {
+    oct_ctx* c = s->ctx;
+    std::vector<float4> h(s->n_nodes);
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    OCT_CUDA(c, cudaMemcpy(h.data(), d, sizeof(float4) * s->n_nodes, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < s->n_nodes; ++i) {
+        if (add_rest) {
+            out[3 * i] = s->X[3 * i] + h[i].x; out[3 * i + 1] = s->X[3 * i + 1] + h[i].y; out[3 * i + 2] = s->X[3 * i + 2] + h[i].z;
+        } else {
+            out[3 * i] = h[i].x; out[3 * i + 1] = h[i].y; out[3 * i + 2] = h[i].z;
+        }
+    }
+    return OCT_OK;
+}
+
+}  // namespace
+
+// ============================================================================ C ABI
+extern "C" {
+
+void oct_desc_init(oct_scene_desc* d) {
+    std::memset(d, 0, sizeof(*d));
+    d->solver = OCT_SOLVER_VBD;
+    d->element = OCT_TETRA;
+    d->density = 1000.f;
+    d->mass_distribution = OCT_MASS_FEMSHAPE;
+    d->material = OCT_STABLE_NEOHOOKE;
+    d->young = 1e6f;
+    d->poisson = 0.45f;
+    d->gravity[1] = -9.81f;
+    d->iterations = 1;
+    d->vbd_version = OCT_VBD_REDUCTION_SYMMETRY;
+    d->target_color = -1;
+    d->color_algo = OCT_COLOR_DSAT;
+    d->precision = OCT_PREC_PLAIN;
+    for (int k = 0; k < 3; ++k) { d->box_min[k] = -1e30f; d->box_max[k] = 1e30f; }
+}
+
+oct_status oct_ctx_create(int device, size_t budget, oct_ctx** out) {
+    if (!out) return OCT_EINVAL;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) return OCT_ECUDA;
+    if (device < 0 || device >= n) return OCT_EINVAL;
+    if (cudaSetDevice(device) != cudaSuccess) return OCT_ECUDA;
+    auto* c = new oct_ctx();
+    c->device = device;
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    c->budget = budget ? budget : (size_t)(0.9 * (double)fr);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess || cudaMalloc(&c->d_error, sizeof(int)) != cudaSuccess ||
+        cudaMemset(c->d_error, 0, sizeof(int)) != cudaSuccess || cudaEventCreate(&c->ev0) != cudaSuccess ||
+        cudaEventCreate(&c->ev1) != cudaSuccess) {
+        delete c;
+        return OCT_ECUDA;
+    }
+    *out = c;
+    return OCT_OK;
+}
+
+oct_status oct_ctx_destroy(oct_ctx* c) {
+    if (!c) return OCT_EINVAL;
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_error);
+    cudaEventDestroy(c->ev0);
+    cudaEventDestroy(c->ev1);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return OCT_OK;
+}
+
+const char* oct_last_error(oct_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+oct_status oct_ctx_memory(oct_ctx* c, size_t* used, size_t* budget) {
+    if (!c) return OCT_EINVAL;
+    if (used) *used = c->used;
+    if (budget) *budget = c->budget;
+    return OCT_OK;
+}
+
+oct_status oct_scene_create(oct_ctx* c, const oct_scene_desc* d, oct_scene** out) {
+    if (!c || !d || !out) return OCT_EINVAL;
+    *out = nullptr;
+    cudaSetDevice(c->device);
+    auto* s = new oct_scene();
+    oct_status st = build_scene(c, d, s);
+    if (st) { s->mem.release(); delete s; return st; }
+    *out = s;
+    return OCT_OK;
+}
+
+oct_status oct_scene_destroy(oct_scene* s) {
+    if (!s) return OCT_EINVAL;
+    cudaStreamSynchronize(s->ctx->stream);
+    s->mem.release();
+    delete s;
+    return OCT_OK;
+}
+
+oct_status oct_scene_step(oct_scene* s, float frame_dt, int substeps) {
+    if (!s || substeps <= 0 || !(frame_dt > 0.f)) return OCT_EINVAL;
+    oct_ctx* c = s->ctx;
+    const float sub = frame_dt / (float)substeps;
+    cudaEventRecord(c->ev0, c->stream);
+    for (int k = 0; k < substeps; ++k) {
+        if (s->solver == OCT_SOLVER_VBD) vbd_substep(s, sub);
+        else if (s->solver == OCT_SOLVER_XPBD) xpbd_substep(s, sub);
+        else explicit_substep(s, sub);
+    }
+    cudaEventRecord(c->ev1, c->stream);
+    OCT_CUDA(c, cudaGetLastError());
+    return OCT_OK;
+}
+
+oct_status oct_scene_sync(oct_scene* s) {
+    if (!s) return OCT_EINVAL;
+    oct_ctx* c = s->ctx;
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1);
+    return check_error_word(c);
+}
+
+oct_status oct_scene_get_positions(oct_scene* s, float* out) {
+    if (!s || !out) return OCT_EINVAL;
+    return read_nodes(s, s->h.u, out, true);
+}
+oct_status oct_scene_get_velocities(oct_scene* s, float* out) {
+    if (!s || !out) return OCT_EINVAL;
+    return read_nodes(s, s->h.v, out, false);
+}
+oct_status oct_scene_set_positions(oct_scene* s, const float* in) {
+    if (!s || !in) return OCT_EINVAL;
+    std::vector<float4> h(s->n_nodes);
+    for (int i = 0; i < s->n_nodes; ++i)
+        h[i] = make_float4(in[3 * i] - s->X[3 * i], in[3 * i + 1] - s->X[3 * i + 1], in[3 * i + 2] - s->X[3 * i + 2], 0.f);
+    OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    OCT_CUDA(s->ctx, cudaMemcpy(s->h.u, h.data(), sizeof(float4) * s->n_nodes, cudaMemcpyHostToDevice));
+    return OCT_OK;
+}
+oct_status oct_scene_set_velocities(oct_scene* s, const float* in) {
+    if (!s || !in) return OCT_EINVAL;
+    std::vector<float4> h(s->n_nodes);
+    for (int i = 0; i < s->n_nodes; ++i) h[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.f);
+    OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    OCT_CUDA(s->ctx, cudaMemcpy(s->h.v, h.data(), sizeof(float4) * s->n_nodes, cudaMemcpyHostToDevice));
+    return OCT_OK;
+}
+
+oct_status oct_scene_info(oct_scene* s, int32_t* nn, int32_t* ne, int32_t* nc, int32_t* nf) {
+    if (!s) return OCT_EINVAL;
+    if (nn) *nn = s->n_nodes;
+    if (ne) *ne = s->n_elements;
+    if (nc) *nc = s->n_colors;
+    if (nf) *nf = s->n_fixed;
+    return OCT_OK;
+}
+
+oct_status oct_scene_get_coloring(oct_scene* s, int32_t* colors, int32_t* order) {
+    if (!s) return OCT_EINVAL;
+    if (colors) std::copy(s->colors.begin(), s->colors.end(), colors);
+    if (order) std::copy(s->vids.begin(), s->vids.end(), order);
+    return OCT_OK;
+}
+
+oct_status oct_scene_get_masses(oct_scene* s, float* out) {
+    if (!s || !out) return OCT_EINVAL;
+    std::copy(s->masses.begin(), s->masses.end(), out);
+    return OCT_OK;
+}
+
+oct_status oct_scene_set_fixation(oct_scene* s, const float offset[3], const float rotation[9]) {
+    if (!s) return OCT_EINVAL;
+    if (offset) { s->h.offx = offset[0]; s->h.offy = offset[1]; s->h.offz = offset[2]; }
+    if (rotation) std::copy(rotation, rotation + 9, s->h.rot);
+    OCT_CUDA(s->ctx, cudaMemcpyAsync(s->d_scene, &s->h, sizeof(SceneDev), cudaMemcpyHostToDevice, s->ctx->stream));
+    OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    return OCT_OK;
+}
+
+oct_status oct_scene_set_precision(oct_scene* s, int precision) {
+    if (!s || precision < 0 || precision > 1) return OCT_EINVAL;
+    s->precision = precision;
+    s->h.precision = precision;
+    OCT_CUDA(s->ctx, cudaMemcpyAsync(s->d_scene, &s->h, sizeof(SceneDev), cudaMemcpyHostToDevice, s->ctx->stream));
+    OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    return OCT_OK;
+}
+
+oct_status oct_scene_energy(oct_scene* s, double out[4]) {
+    if (!s || !out) return OCT_EINVAL;
+    oct_ctx* c = s->ctx;
+    OCT_CUDA(c, cudaMemsetAsync(s->d_red, 0, 4 * sizeof(double), c->stream));
+    launch_energy(s->element, s->material, s->d_scene, 0, s->n_nodes, s->n_elements, s->d_red, c->d_error, c->stream);
+    OCT_CUDA(c, cudaMemcpyAsync(out, s->d_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    out[3] = out[0] + out[1] + out[2];
+    return check_error_word(c);
+}
+
+oct_status oct_scene_residual(oct_scene* s, float dt, double out[2]) {
+    if (!s || !out || !(dt > 0.f)) return OCT_EINVAL;
+    if (s->solver != OCT_SOLVER_VBD) return OCT_ENOTSUP;
+    oct_ctx* c = s->ctx;
+    StepParams P = base_params(c, dt);
+    OCT_CUDA(c, cudaMemsetAsync(s->d_red, 0, 4 * sizeof(double), c->stream));
+    for (int k = 0; k < s->n_colors; ++k) {
+        const int b = s->vwork_off[k], n = s->vwork_off[k + 1] - b;
+        launch_vertex(s->element, s->material, s->d_scene, s->d_vwork + b, n, s->tpv, 1, P, s->d_red, c->stream);
+    }
+    OCT_CUDA(c, cudaMemcpyAsync(out, s->d_red, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_error_word(c);
+}
+
+oct_status oct_ctx_stream(oct_ctx* c, void** stream) {
+    if (!c || !stream) return OCT_EINVAL;
+    *stream = (void*)c->stream;
+    return OCT_OK;
+}
+
+oct_status oct_fp32_peak(oct_ctx* c, double* tflops) {
+    if (!c || !tflops) return OCT_EINVAL;
+    launch_fma_peak(c->stream);   // warm-up
+    OCT_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    double fmas = 0;
+    for (int k = 0; k < 5; ++k) fmas += launch_fma_peak(c->stream);
+    OCT_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    OCT_CUDA(c, cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    *tflops = 2.0 * fmas / (ms * 1e-3) / 1e12;
+    return OCT_OK;
+}
+
+oct_status oct_last_step_ms(oct_ctx* c, float* ms) {
+    if (!c || !ms) return OCT_EINVAL;
+    *ms = c->last_ms;
+    return OCT_OK;
+}
+
+oct_status oct_launch_count(oct_ctx* c, uint64_t* n) {
+    if (!c || !n) return OCT_EINVAL;
+    *n = c->launches;
+    return OCT_OK;
+}
+
+// ---------------------------------------------------------------------------- batches
+oct_status oct_batch_create(oct_ctx* c, oct_scene* const* scenes, int n, oct_batch** out) {
+    if (!c || !scenes || n <= 0 || !out) return OCT_EINVAL;
+    *out = nullptr;
+    auto b = std::make_unique<oct_batch>();
+    b->ctx = c;
+    b->mem.ctx = c;
+    b->iterations = scenes[0]->iterations;
+    b->rho = scenes[0]->rho;
+    std::vector<SceneDev> hs;
+    std::vector<NWork> nw, fw, bw;
+    std::map<std::pair<std::pair<int, int>, std::pair<int, int>>, int> gid;
+    std::vector<std::vector<std::vector<VWork>>> gwork;   // group -> colour -> items
+    size_t off = 0;
+    for (int i = 0; i < n; ++i) {
+        oct_scene* s = scenes[i];
+        if (!s || s->ctx != c) return fail(c, OCT_EINVAL, "scene from another context");
+        if (s->solver != OCT_SOLVER_VBD) return fail(c, OCT_ENOTSUP, "batches hold VBD scenes");
+        if (s->iterations != b->iterations || s->rho != b->rho) return fail(c, OCT_ENOTSUP, "batch scenes need equal iterations and rho");
+        if (s->order_mode != OCT_ORDER_ASCENDING) return fail(c, OCT_ENOTSUP, "batches use the ascending colour order");
+        b->scenes.push_back(s);
+        hs.push_back(s->h);
+        b->pending_host.push_back(s->pending_host);
+        b->state_off.push_back(off);
+        off += (size_t)s->n_nodes * 6;
+        auto key = std::make_pair(std::make_pair(s->element, s->material), std::make_pair(s->tpv, s->in_place ? 1 : 0));
+        auto it = gid.find(key);
+        if (it == gid.end()) {
+            it = gid.emplace(key, (int)b->groups.size()).first;
+            oct_batch::Group g;
+            g.element = s->element; g.material = s->material; g.tpv = s->tpv; g.in_place = s->in_place;
+            b->groups.push_back(g);
+            gwork.emplace_back();
+        }
+        auto& cw = gwork[it->second];
+        if ((int)cw.size() < s->n_colors) cw.resize(s->n_colors);
+        for (int k = 0; k < s->n_colors; ++k) append_vwork(cw[k], i, s->color_off[k], s->color_off[k + 1], s->tpv);
+        append_nwork(nw, i, s->n_nodes);
+        std::vector<NWork> f1;
+        append_nwork(f1, i, s->n_fixed);
+        fw.insert(fw.end(), f1.begin(), f1.end());
+        if (s->box) append_nwork(bw, i, s->n_nodes);
+    }
+    b->state_off.push_back(off);
+    std::vector<VWork> all;
+    for (size_t g = 0; g < b->groups.size(); ++g) {
+        b->groups[g].base = (int)all.size();
+        b->groups[g].off.assign(1, 0);
+        for (auto& items : gwork[g]) {
+            all.insert(all.end(), items.begin(), items.end());
+            b->groups[g].off.push_back((int)(all.size() - b->groups[g].base));
+        }
+        OCT_CUDA(c, cudaStreamCreateWithFlags(&b->groups[g].stream, cudaStreamNonBlocking));
+        OCT_CUDA(c, cudaEventCreateWithFlags(&b->groups[g].done, cudaEventDisableTiming));
+    }
+    OCT_CUDA(c, cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    oct_status st;
+    if ((st = upload(c, b->mem, b->d_scenes, hs)) || (st = upload(c, b->mem, b->d_vwork, all)) ||
+        (st = upload(c, b->mem, b->d_nwork, nw)) || (st = upload(c, b->mem, b->d_fwork, fw)) ||
+        (st = upload(c, b->mem, b->d_bwork, bw)) || (st = upload(c, b->mem, b->d_pending, b->pending_host))) {
+        b->mem.release();
+        return st;
+    }
+    b->n_nwork = (int)nw.size();
+    b->n_fwork = (int)fw.size();
+    b->n_bwork = (int)bw.size();
+    *out = b.release();
+    return OCT_OK;
+}
+
+namespace {
+// Enqueue one sub-step of the whole batch on the context stream (captured into a graph).
+void batch_substep(oct_batch* b, float dt) {
+    oct_ctx* c = b->ctx;
+    cudaStream_t st = c->stream;
+    StepParams P = base_params(c, dt);
+    P.pending_v0 = b->d_pending;
+    const bool cheb = b->rho > 0.f && b->rho > 1.17549435e-38f * 1e6f;
+    launch_predict(b->d_scenes, b->d_nwork, b->n_nwork, 0, 0, cheb ? 1 : 0, P, st);
+    cudaMemsetAsync(b->d_pending, 0, sizeof(int) * b->scenes.size(), st);
+    float omega = 1.f;
+    for (int j = 0; j < b->iterations; ++j) {
+        cudaEventRecord(b->fork, st);
+        for (auto& g : b->groups) {
+            cudaStreamWaitEvent(g.stream, b->fork, 0);
+            StepParams Pg = P;
+            Pg.in_place = g.in_place ? 1 : 0;
+            for (size_t k = 0; k + 1 < g.off.size(); ++k) {
+                const VWork* w = b->d_vwork + g.base + g.off[k];
+                const int n = g.off[k + 1] - g.off[k];
+                launch_vertex(g.element, g.material, b->d_scenes, w, n, g.tpv, 0, Pg, nullptr, g.stream);
+                if (!g.in_place) launch_commit(b->d_scenes, w, n, g.stream);
+            }
+            cudaEventRecord(g.done, g.stream);
+            cudaStreamWaitEvent(st, g.done, 0);
+        }
+        if (b->n_fwork) launch_constraints(b->d_scenes, b->d_fwork, b->n_fwork, 0, st);
+        if (b->n_bwork) launch_constraints(b->d_scenes, b->d_bwork, b->n_bwork, 1, st);
+        if (cheb) {
+            if (j == 1) omega = 2.f / (2.f - b->rho * b->rho);
+            else if (j > 1) omega = 4.f / (4.f - b->rho * b->rho * omega);
+            P.omega = omega;
+            P.iteration = j;
+            launch_chebyshev(b->d_scenes, b->d_nwork, b->n_nwork, P, st);
+        }
+    }
+    launch_velocity(b->d_scenes, b->d_nwork, b->n_nwork, 0.f, 0, P, st);
+}
+
+uint64_t batch_launches_per_substep(const oct_batch* b) {
+    uint64_t n = 2;
+    for (auto& g : b->groups) n += (uint64_t)(g.off.size() - 1) * (g.in_place ? 1 : 2) * b->iterations;
+    if (b->n_fwork) n += b->iterations;
+    if (b->n_bwork) n += b->iterations;
+    if (b->rho > 0.f) n += b->iterations;
+    return n;
+}
+}  // namespace
+
+oct_status oct_batch_step(oct_batch* b, float frame_dt, int substeps) {
+    if (!b || substeps <= 0 || !(frame_dt > 0.f)) return OCT_EINVAL;
+    oct_ctx* c = b->ctx;
+    const float sub = frame_dt / (float)substeps;
+    if (!b->exec || b->graph_dt != sub) {
+        if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+        if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+        OCT_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        batch_substep(b, sub);
+        OCT_CUDA(c, cudaStreamEndCapture(c->stream, &b->graph));
+        OCT_CUDA(c, cudaGraphInstantiate(&b->exec, b->graph, 0));
+        b->graph_dt = sub;
+    }
+    cudaEventRecord(c->ev0, c->stream);
+    for (int k = 0; k < substeps; ++k) {
+        OCT_CUDA(c, cudaGraphLaunch(b->exec, c->stream));
+        c->launches += batch_launches_per_substep(b);
+    }
+    cudaEventRecord(c->ev1, c->stream);
+    for (auto* s : b->scenes) s->pending_host = 0;
+    return OCT_OK;
+}
+
+oct_status oct_batch_destroy(oct_batch* b) {
+    if (!b) return OCT_EINVAL;
+    cudaStreamSynchronize(b->ctx->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (auto& g : b->groups) { cudaStreamDestroy(g.stream); cudaEventDestroy(g.done); }
+    if (b->fork) cudaEventDestroy(b->fork);
+    b->mem.release();
+    delete b;
+    return OCT_OK;
+}
+
+oct_status oct_batch_group_info(oct_batch* b, int g, int32_t* element, int32_t* material, double* flops, double* bytes,
+                                int32_t* launches, int64_t* vertices) {
+    if (!b || g < 0 || g >= (int)b->groups.size()) return OCT_EINVAL;
+    const auto& G = b->groups[g];
+    // Algorithmic work of one sweep: every free vertex of every scene of the group once.
+    // flops: per (owner, quadrature point) term vbd_term_flops; bytes: per vertex u, u_last,
+    // y read + u written (16 B each) + mask/slot/owner-offset ints, per owner entry 4 B,
+    // per element its topology (4 NE) and quadrature records (48 NQ) once.
+    double fl = 0, by = 0;
+    int64_t nv = 0;
+    const double tf = vbd_term_flops(G.element, G.material);
+    for (auto* s : b->scenes) {
+        if (s->element != G.element || s->material != G.material || s->tpv != G.tpv || s->in_place != G.in_place) continue;
+        const int64_t free_nodes = s->n_nodes - s->n_fixed;
+        const int64_t terms = (int64_t)s->n_elements * s->ne * s->nq;   // sum over vertices of owners x Q
+        fl += tf * (double)terms * (double)free_nodes / (double)s->n_nodes;
+        by += (double)s->n_nodes * (4 * 16 + 12) + (double)s->n_elements * s->ne * 4.0 +
+              (double)s->n_elements * (4.0 * s->ne + 48.0 * s->nq);
+        nv += free_nodes;
+    }
+    if (element) *element = G.element;
+    if (material) *material = G.material;
+    if (flops) *flops = fl;
+    if (bytes) *bytes = by;
+    if (launches) *launches = (int32_t)(G.off.size() - 1) * (G.in_place ? 1 : 2);
+    if (vertices) *vertices = nv;
+    return OCT_OK;
+}
+
+oct_status oct_batch_time_group(oct_batch* b, int g, int sweeps, float dt, float* ms) {
+    if (!b || g < 0 || g >= (int)b->groups.size() || sweeps <= 0 || !ms || !(dt > 0.f)) return OCT_EINVAL;
+    oct_ctx* c = b->ctx;
+    const auto& G = b->groups[g];
+    StepParams P = base_params(c, dt);
+    P.in_place = G.in_place ? 1 : 0;
+    OCT_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    for (int r = 0; r < sweeps; ++r)
+        for (size_t k = 0; k + 1 < G.off.size(); ++k) {
+            const VWork* w = b->d_vwork + G.base + G.off[k];
+            const int n = G.off[k + 1] - G.off[k];
+            launch_vertex(G.element, G.material, b->d_scenes, w, n, G.tpv, 0, P, nullptr, c->stream);
+            if (!G.in_place) launch_commit(b->d_scenes, w, n, c->stream);
+            c->launches += G.in_place ? 1 : 2;
+        }
+    OCT_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    OCT_CUDA(c, cudaEventSynchronize(c->ev1));
+    OCT_CUDA(c, cudaGetLastError());
+    cudaEventElapsedTime(ms, c->ev0, c->ev1);
+    return OCT_OK;
+}
+
+oct_status oct_batch_state_size(oct_batch* b, size_t* n) {
+    if (!b || !n) return OCT_EINVAL;
+    *n = b->state_off.back();
+    return OCT_OK;
+}
+
+// Host <-> device state transfer of a batch: per scene n*3 displacements (p - X) then n*3
+// velocities, each moved with one strided copy into the float4 node arrays
+// (cudaMemcpy2DAsync: 12 of every 16 bytes).
+oct_status oct_batch_set_state(oct_batch* b, const float* host) {
+    if (!b || !host) return OCT_EINVAL;
+    oct_ctx* c = b->ctx;
+    for (size_t i = 0; i < b->scenes.size(); ++i) {
+        oct_scene* s = b->scenes[i];
+        const float* p = host + b->state_off[i];
+        const float* v = p + 3 * (size_t)s->n_nodes;
+        OCT_CUDA(c, cudaMemcpy2DAsync(s->h.u, sizeof(float4), p, 3 * sizeof(float), 3 * sizeof(float), s->n_nodes,
+                                      cudaMemcpyHostToDevice, c->stream));
+        OCT_CUDA(c, cudaMemcpy2DAsync(s->h.v, sizeof(float4), v, 3 * sizeof(float), 3 * sizeof(float), s->n_nodes,
+                                      cudaMemcpyHostToDevice, c->stream));
+    }
+    return OCT_OK;
+}
+
+oct_status oct_batch_get_state(oct_batch* b, float* host) {
+    if (!b || !host) return OCT_EINVAL;
+    oct_ctx* c = b->ctx;
+    for (size_t i = 0; i < b->scenes.size(); ++i) {
+        oct_scene* s = b->scenes[i];
+        float* p = host + b->state_off[i];
+        float* v = p + 3 * (size_t)s->n_nodes;
+        OCT_CUDA(c, cudaMemcpy2DAsync(p, 3 * sizeof(float), s->h.u, sizeof(float4), 3 * sizeof(float), s->n_nodes,
+                                      cudaMemcpyDeviceToHost, c->stream));
+        OCT_CUDA(c, cudaMemcpy2DAsync(v, 3 * sizeof(float), s->h.v, sizeof(float4), 3 * sizeof(float), s->n_nodes,
+                                      cudaMemcpyDeviceToHost, c->stream));
+    }
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return OCT_OK;
+}
+
+}  // extern "C"

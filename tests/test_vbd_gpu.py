@@ -1,0 +1,122 @@
+"""GPU parity of the VBD colour sweep against the CPU oracle, through the C ABI.
+
+Tolerances (FP32): node positions after one step within 1e-5 of the positions' magnitude
+(relative max-norm) against the FP32 oracle, the same against the FP64 oracle, and the
+total-energy trace over 100 steps within 1e-3 relative.  Colouring and vertex order are
+compared bit for bit."""
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from scenes import disp_err, pair, rel_err
+
+pytestmark = pytest.mark.gpu
+ELEMS = [O.TETRA, O.HEXA, O.TETRA10, O.TETRA20, O.HEXA27]
+
+
+def test_config1_one_step_and_colouring(ctx):
+    """Config 1: 8x2x2 P1 beam, Stable NH E=1e5 nu=0.45 rho=1000, 1 substep x 20 iterations."""
+    s, o32, o64, mesh = pair(ctx, O.TETRA, cells=(8, 2, 2), size=(1.0, 0.25, 0.25), iterations=20)
+    c, order = s.coloring()
+    assert np.array_equal(c, mesh["colors"])
+    ref_order = np.concatenate([np.nonzero(mesh["colors"] == k)[0] for k in range(mesh["n_colors"])])
+    assert np.array_equal(order, ref_order)
+    assert np.array_equal(s.masses(), mesh["m"])
+    s.step(0.01, 1)
+    o32.step(0.01, 1)
+    o64.step(0.01, 1)
+    p = s.get_position()
+    assert rel_err(p, o32.get(0)) < 1e-5
+    assert rel_err(p, o64.get(0)) < 1e-5
+    assert disp_err(p, o64.get(0), mesh["X"]) < 1e-3
+
+
+@pytest.mark.parametrize("element", ELEMS)
+@pytest.mark.parametrize("material", [O.STABLE_NEOHOOKE, O.NEOHOOKE, O.STVK, O.HOOKE])
+def test_one_step_parity_all_elements_materials(ctx, element, material):
+    cells = (3, 2, 2) if element in (O.TETRA20, O.HEXA27) else (4, 2, 2)
+    s, o32, o64, mesh = pair(ctx, element, cells=cells, material=material, iterations=5, young=2e5, damping=1e-3)
+    s.step(1 / 60, 2)
+    o32.step(1 / 60, 2)
+    o64.step(1 / 60, 2)
+    p = s.get_position()
+    assert rel_err(p, o32.get(0)) < 1e-5, (rel_err(p, o32.get(0)), disp_err(p, o32.get(0), mesh["X"]))
+    assert rel_err(p, o64.get(0)) < 1e-5
+    v = s.get_velocity()
+    assert np.abs(v - o64.get(1)).max() < 1e-3 * max(1.0, np.abs(o64.get(1)).max())
+
+
+def test_energy_trace_100_steps_config1(ctx):
+    s, o32, o64, mesh = pair(ctx, O.TETRA, cells=(8, 2, 2), size=(1.0, 0.25, 0.25), iterations=20)
+    eg, eo = [], []
+    for _ in range(100):
+        s.step(0.01, 1)
+        o64.step(0.01, 1)
+        eg.append(s.energy()[3])
+        eo.append(o64.energy()[3])
+    eg, eo = np.array(eg), np.array(eo)
+    scale = np.abs(eo).max()
+    assert np.abs(eg - eo).max() / scale < 1e-3
+    assert rel_err(s.get_position(), o64.get(0)) < 1e-4
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_mixed_precision_closer_to_fp64(ctx, precision):
+    s, o32, o64, mesh = pair(ctx, O.TETRA10, cells=(6, 2, 2), size=(2.0, 0.5, 0.5), iterations=10, young=1e6,
+                             poisson=0.49, density=1100.0, precision=precision)
+    for _ in range(3):
+        s.step(1 / 60, 5)
+        o64.step(1 / 60, 5)
+    assert disp_err(s.get_position(), o64.get(0), mesh["X"]) < 1e-2
+
+
+def test_jacobi_colour_reduction_matches_oracle(ctx):
+    """Better_Coloration with a target below the DSAT count: conflicts inside colours, so
+    each colour updates from the same state (kernel_vbd_solve_v4 + copy)."""
+    s, o32, o64, mesh = pair(ctx, O.TETRA10, cells=(4, 2, 2), iterations=6, version=3, target=6)
+    assert s.n_colors == 6
+    s.step(1 / 60, 2)
+    o64.step(1 / 60, 2)
+    assert rel_err(s.get_position(), o64.get(0)) < 1e-5
+
+
+def test_initial_velocity_and_chebyshev(ctx):
+    X_probe = O.beam_mesh(O.HEXA, (4, 2, 2), (1.0, 0.25, 0.25))[0]
+    rng = np.random.default_rng(7)
+    v0 = rng.normal(0, 0.05, size=X_probe.shape).astype(np.float32)
+    s, o32, o64, mesh = pair(ctx, O.HEXA, cells=(4, 2, 2), iterations=8, v0=v0, rho=0.7)
+    for _ in range(3):
+        s.step(1 / 60, 2)
+        o64.step(1 / 60, 2)
+    assert rel_err(s.get_position(), o64.get(0)) < 1e-5
+
+
+@pytest.mark.parametrize("tpv", [1, 2, 4, 16, 32])
+def test_threads_per_vertex_do_not_change_results(ctx, tpv):
+    s, o32, o64, mesh = pair(ctx, O.TETRA, cells=(6, 2, 2), iterations=5, tpv=tpv)
+    s.step(0.01, 1)
+    o64.step(0.01, 1)
+    assert rel_err(s.get_position(), o64.get(0)) < 1e-5
+
+
+def test_per_element_young_and_box_limit(ctx):
+    X, T = O.beam_mesh(O.TETRA, (6, 2, 2), (1.0, 0.25, 0.25))
+    E = np.exp(np.random.default_rng(3).uniform(np.log(1e4), np.log(1e6), len(T))).astype(np.float32)
+    box = ((-1.0, -1.0, -0.02), (2.0, 1.0, 1.0))
+    s, o32, o64, mesh = pair(ctx, O.TETRA, cells=(6, 2, 2), iterations=5, young_per_element=E, box=box)
+    for _ in range(5):
+        s.step(0.01, 1)
+        o64.step(0.01, 1)
+    p = s.get_position()
+    assert rel_err(p, o64.get(0)) < 1e-5
+    assert p[:, 2].min() >= -0.02 - 1e-6
+
+
+def test_residual_and_energy_are_finite_and_decrease(ctx):
+    s, o32, o64, mesh = pair(ctx, O.TETRA, cells=(8, 2, 2), size=(1.0, 0.25, 0.25), iterations=1)
+    s.step(0.01, 1)
+    r1 = s.residual(0.01)
+    o64.step(0.01, 1)
+    ro = o64.residual(0.01)
+    assert np.isfinite(r1).all()
+    assert abs(r1[0] - ro[0]) / max(ro[0], 1e-30) < 1e-3
