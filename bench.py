@@ -55,13 +55,13 @@ def workload_specs(name, seed):
     raise SystemExit("unknown workload " + name)
 
 
-def build_scene(ctx, spec, iterations, precision, seed):
+def build_scene(ctx, spec, iterations, precision, seed, tpv=0):
     import octopusengine_b200 as ob
     X, T = ob.beam_mesh(spec["element"], spec["cells"], spec["size"])
     fixed = ob.fixed_by_plane(X, (0.01, 0.0, 0.0), (-1.0, 0.0, 0.0))
     kw = dict(density=spec["density"], mass_distribution=ob.MASS_FEMSHAPE, material=ob.STABLE_NEOHOOKE,
               young=spec["young"], poisson=spec["poisson"], fixed_ids=fixed, iterations=iterations,
-              gravity=(0.0, 0.0, -9.81), precision=precision)
+              gravity=(0.0, 0.0, -9.81), precision=precision, threads_per_vertex=tpv)
     if spec.get("v0_sigma"):
         kw["initial_velocity"] = np.random.default_rng(seed).normal(0, spec["v0_sigma"], X.shape).astype(np.float32)
     return ob.Scene(ctx, spec["element"], X, T, **kw)
@@ -134,7 +134,7 @@ def cpu_reference(specs, iterations, substeps, dt, threads, sample_every, sample
         keep.append(s)
         solvers.append(O.CpuVBD(s))
         vit += (len(X) - len(fixed)) * sample_iters
-    secs = O.run_cpu_many(solvers, dt, 1, True, threads)
+    secs = O.run_cpu_many(solvers, dt / substeps, 1, True, threads)
     desc = ("%d of %d scenes (every %d-th), 1 sub-step x %d iterations of dt=%.5f s, %d host threads, "
             "reference CPU VBD restated in C++ (oracle/), per-iteration force pass included"
             % (len(sel), len(specs), sample_every, sample_iters, dt / substeps, threads))
@@ -151,6 +151,7 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tpv", type=int, default=0, help="threads per vertex (0 = per-element default)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -167,7 +168,7 @@ def main():
         its = 4 if args.workload == "batched" else (2 if args.workload == "p2" else iterations)
         vals = []
         for _ in range(args.warmup + args.steps):
-            v, secs, desc = cpu_reference(specs, iterations, substeps, frame_dt / substeps * substeps, threads, every, its)
+            v, secs, desc = cpu_reference(specs, iterations, substeps, frame_dt, threads, every, its)
             vals.append(v)
         v = float(np.median(vals[args.warmup:]))
         line = {"impl": "reference", "metric": "vertex_iterations_per_s", "value": v, "unit": "vertex-iter/s",
@@ -196,7 +197,7 @@ def main():
     # scene set-up (host colouring etc.) in parallel host threads
     t0 = time.time()
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
-        scenes = list(ex.map(lambda a: build_scene(ctx, a[1], iterations, ob.PREC_MIXED, args.seed + a[0]),
+        scenes = list(ex.map(lambda a: build_scene(ctx, a[1], iterations, ob.PREC_MIXED, args.seed + a[0], args.tpv),
                              enumerate(specs)))
     setup_s = time.time() - t0
     batch = ob.Batch(ctx, scenes)

@@ -167,6 +167,45 @@ oct_status oct_shape_table(int element, int32_t* n_quadrature, double* coords, d
 oct_status oct_color(int element, const int32_t* topology, int n_elements, int n_nodes, int algo, int target,
                      int32_t* colors, int32_t* n_colors, int64_t* conflicts);
 
+/* Device bytes a scene built from desc will hold (estimate used for HBM admission). */
+oct_status oct_scene_footprint(const oct_scene_desc* desc, size_t* bytes);
+
+/* Serving loop: continuous batching of (scene, steps) requests on one device.  Requests are
+ * admitted while HBM budget and slots allow; the host set-up of newly admitted scenes runs
+ * on worker threads while the GPU advances the active batch, and admitted scenes join the
+ * batch at the next frame boundary; finished scenes leave it and free their memory.  Every
+ * frame advances all active scenes by frame_dt (substeps x iterations VBD). */
+typedef struct oct_server_config {
+    size_t hbm_budget;        /* bytes of scene state the server may hold (0 = context budget) */
+    int32_t max_scenes;       /* active slots */
+    float frame_dt;
+    int32_t substeps;
+    int32_t iterations;       /* overrides desc->iterations of submitted scenes */
+    int32_t precision;        /* OCT_PREC_* for submitted scenes */
+    int32_t setup_threads;    /* host threads for scene set-up (0 = hardware concurrency) */
+} oct_server_config;
+
+typedef struct oct_server_stats {
+    int64_t submitted, admitted, finished, rejected, queued, active;
+    int64_t frames;
+    double p50_step_ms, p99_step_ms, mean_step_ms;   /* device time of a batched frame */
+    double vertex_iterations;                         /* total free-vertex updates done */
+    double busy_ms;                                   /* summed device time of the frames */
+    size_t bytes_in_use;
+} oct_server_stats;
+
+oct_status oct_server_create(oct_ctx* ctx, const oct_server_config* cfg, oct_server** out);
+/* Queues a request; the desc and its arrays are copied.  OCT_ENOMEM_BUDGET if the scene can
+ * never fit the server budget (the request is rejected, nothing is queued). */
+oct_status oct_server_submit(oct_server* srv, const oct_scene_desc* desc, int32_t steps, int64_t* request_id);
+/* One scheduling round: start admissions that fit, run one batched frame of the active
+ * scenes, retire finished requests.  Returns the number of active scenes after the frame. */
+oct_status oct_server_tick(oct_server* srv, int32_t* n_active);
+/* done = 1 when the request has finished; then positions (n_nodes*3, may be NULL) are copied out. */
+oct_status oct_server_poll(oct_server* srv, int64_t request_id, int32_t* done, float* positions);
+oct_status oct_server_get_stats(oct_server* srv, oct_server_stats* out);
+oct_status oct_server_destroy(oct_server* srv);
+
 /* Measurement helpers.  The context's CUDA stream (cudaStream_t), to record events on it. */
 oct_status oct_ctx_stream(oct_ctx* ctx, void** stream);
 /* Measured FP32 FMA throughput of the device (TFLOP/s) from a register-resident FMA loop. */

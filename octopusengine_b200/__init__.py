@@ -24,7 +24,7 @@ from .capi import (COLOR_DSAT, COLOR_GREEDY, ELEMENT_NODES, HEXA, HEXA27, HOOKE,
                    SOLVER_XPBD, STABLE_NEOHOOKE, STVK, TETRA, TETRA10, TETRA20, VBD_BASE, VBD_BETTER_COLORATION,
                    VBD_REDUCTION_SYMMETRY, OctError, beam_mesh, color, fixed_by_plane, lumped_masses, shape_table)
 
-__all__ = ["Context", "Scene", "Batch", "OctError", "beam_mesh", "color", "lumped_masses", "shape_table",
+__all__ = ["Context", "Scene", "Batch", "Server", "make_desc", "OctError", "beam_mesh", "color", "lumped_masses", "shape_table",
            "fixed_by_plane", "library_path"]
 
 
@@ -72,35 +72,41 @@ class Context:
             pass
 
 
+def make_desc(element, positions, topology, **kw):
+    """Builds an oct_scene_desc; returns (desc, arrays kept alive while the desc is used)."""
+    X = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+    T = np.ascontiguousarray(topology, np.int32).reshape(-1, ELEMENT_NODES[element])
+    d = capi.SceneDesc()
+    capi.lib().oct_desc_init(C.byref(d))
+    keep = [X, T]
+    d.element = element
+    d.n_nodes = len(X)
+    d.positions = capi.ptr(X, C.c_float)
+    d.n_elements = len(T)
+    d.topology = capi.ptr(T, C.c_int32)
+    for k, v in kw.items():
+        if k in ("masses", "young_per_element", "initial_velocity"):
+            a = np.ascontiguousarray(v, np.float32).ravel()
+            keep.append(a)
+            setattr(d, k, capi.ptr(a, C.c_float))
+        elif k == "fixed_ids":
+            a = np.ascontiguousarray(v, np.int32).ravel()
+            keep.append(a)
+            d.fixed_ids = capi.ptr(a, C.c_int32) if len(a) else None
+            d.n_fixed = len(a)
+        elif k in ("gravity", "plane_origin", "plane_normal", "box_min", "box_max"):
+            setattr(d, k, (C.c_float * 3)(*v))
+        else:
+            setattr(d, k, v)
+    return d, keep
+
+
 class Scene:
     """One simulated object.  Keyword arguments map 1:1 onto oct_scene_desc fields."""
 
     def __init__(self, ctx, element, positions, topology, **kw):
         self.ctx = ctx
-        X = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
-        T = np.ascontiguousarray(topology, np.int32).reshape(-1, ELEMENT_NODES[element])
-        d = capi.SceneDesc()
-        capi.lib().oct_desc_init(C.byref(d))
-        keep = [X, T]
-        d.element = element
-        d.n_nodes = len(X)
-        d.positions = capi.ptr(X, C.c_float)
-        d.n_elements = len(T)
-        d.topology = capi.ptr(T, C.c_int32)
-        for k, v in kw.items():
-            if k in ("masses", "young_per_element", "initial_velocity"):
-                a = np.ascontiguousarray(v, np.float32).ravel()
-                keep.append(a)
-                setattr(d, k, capi.ptr(a, C.c_float))
-            elif k == "fixed_ids":
-                a = np.ascontiguousarray(v, np.int32).ravel()
-                keep.append(a)
-                d.fixed_ids = capi.ptr(a, C.c_int32) if len(a) else None
-                d.n_fixed = len(a)
-            elif k in ("gravity", "plane_origin", "plane_normal", "box_min", "box_max"):
-                setattr(d, k, (C.c_float * 3)(*v))
-            else:
-                setattr(d, k, v)
+        d, keep = make_desc(element, positions, topology, **kw)
         self._h = C.c_void_p()
         capi.check(capi.lib().oct_scene_create(ctx.handle, C.byref(d), C.byref(self._h)), "oct_scene_create",
                    ctx.handle)
@@ -209,4 +215,48 @@ class Batch:
     def close(self):
         if self._h:
             capi.lib().oct_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+
+class Server:
+    """Continuous-batching request loop (oct_server_*): submit (scene, steps) requests, tick
+    frames, poll results."""
+
+    def __init__(self, ctx, frame_dt=1 / 60, substeps=4, iterations=20, max_scenes=1024, hbm_budget=0,
+                 precision=PREC_MIXED, setup_threads=0):
+        self.ctx = ctx
+        cfg = capi.ServerConfig(hbm_budget, max_scenes, frame_dt, substeps, iterations, precision, setup_threads)
+        self._h = C.c_void_p()
+        capi.check(capi.lib().oct_server_create(ctx.handle, C.byref(cfg), C.byref(self._h)), "oct_server_create")
+        ctx._objs.append(self)
+        self.n_nodes = {}
+
+    def submit(self, element, positions, topology, steps, **kw):
+        d, keep = make_desc(element, positions, topology, **kw)
+        rid = C.c_int64()
+        capi.check(capi.lib().oct_server_submit(self._h, C.byref(d), steps, C.byref(rid)), "oct_server_submit")
+        self.n_nodes[rid.value] = d.n_nodes
+        return rid.value
+
+    def tick(self):
+        n = C.c_int32()
+        capi.check(capi.lib().oct_server_tick(self._h, C.byref(n)), "oct_server_tick", self.ctx.handle)
+        return n.value
+
+    def poll(self, rid):
+        done = C.c_int32()
+        out = np.zeros((self.n_nodes[rid], 3), np.float32)
+        st = capi.lib().oct_server_poll(self._h, rid, C.byref(done), capi.ptr(out, C.c_float))
+        if st != capi.OK:
+            raise OctError(st, "oct_server_poll")
+        return (out if done.value else None)
+
+    def stats(self):
+        s = capi.ServerStats()
+        capi.check(capi.lib().oct_server_get_stats(self._h, C.byref(s)), "oct_server_get_stats")
+        return {k: getattr(s, k) for k, _ in capi.ServerStats._fields_}
+
+    def close(self):
+        if self._h:
+            capi.lib().oct_server_destroy(self._h)
             self._h = C.c_void_p()

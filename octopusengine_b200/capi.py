@@ -33,8 +33,23 @@ EXPORTS = [
     "oct_scene_residual", "oct_batch_create", "oct_batch_step", "oct_batch_destroy", "oct_batch_set_state",
     "oct_batch_get_state", "oct_batch_state_size", "oct_beam_mesh", "oct_lumped_masses", "oct_shape_table",
     "oct_color", "oct_last_step_ms", "oct_launch_count", "oct_ctx_stream", "oct_fp32_peak",
-    "oct_batch_group_info", "oct_batch_time_group", "oct_scene_set_precision",
+    "oct_batch_group_info", "oct_batch_time_group", "oct_scene_set_precision", "oct_scene_footprint",
+    "oct_server_create", "oct_server_submit", "oct_server_tick", "oct_server_poll", "oct_server_get_stats",
+    "oct_server_destroy",
 ]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget", C.c_size_t), ("max_scenes", C.c_int32), ("frame_dt", C.c_float),
+                ("substeps", C.c_int32), ("iterations", C.c_int32), ("precision", C.c_int32),
+                ("setup_threads", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("finished", C.c_int64),
+                ("rejected", C.c_int64), ("queued", C.c_int64), ("active", C.c_int64), ("frames", C.c_int64),
+                ("p50_step_ms", C.c_double), ("p99_step_ms", C.c_double), ("mean_step_ms", C.c_double),
+                ("vertex_iterations", C.c_double), ("busy_ms", C.c_double), ("bytes_in_use", C.c_size_t)]
 
 
 class SceneDesc(C.Structure):
@@ -107,6 +122,13 @@ def lib():
             "oct_batch_group_info": ([vp, C.c_int, ip, ip, dp, dp, ip, C.POINTER(C.c_int64)], C.c_int),
             "oct_batch_time_group": ([vp, C.c_int, C.c_int, C.c_float, fp], C.c_int),
             "oct_scene_set_precision": ([vp, C.c_int], C.c_int),
+            "oct_scene_footprint": ([C.POINTER(SceneDesc), C.POINTER(C.c_size_t)], C.c_int),
+            "oct_server_create": ([vp, C.POINTER(ServerConfig), pp], C.c_int),
+            "oct_server_submit": ([vp, C.POINTER(SceneDesc), C.c_int32, C.POINTER(C.c_int64)], C.c_int),
+            "oct_server_tick": ([vp, ip], C.c_int),
+            "oct_server_poll": ([vp, C.c_int64, ip, fp], C.c_int),
+            "oct_server_get_stats": ([vp, C.POINTER(ServerStats)], C.c_int),
+            "oct_server_destroy": ([vp], C.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)

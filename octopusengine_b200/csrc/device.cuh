@@ -52,12 +52,15 @@ struct SceneDev {
     int precision;                     // 0 plain, 1 mixed
 };
 
-// One block-sized unit of colour work: `count` consecutive colour slots of one scene.
+// One unit of colour work: `count` consecutive colour slots of one scene.  With a fixed
+// number of lanes per vertex an item fills one block (128 / lanes slots); in the packed
+// mapping an item fills one warp (one lane per (vertex, owner) pair, at most 32 pairs) and
+// pair_base is the owner-CSR offset of its first slot.
 struct VWork {
     int scene;
     int slot_begin;
     int count;
-    int pad;
+    int pair_base;
 };
 
 // One unit of node-parallel work (predictor, velocity update, Chebyshev).

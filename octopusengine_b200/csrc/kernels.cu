@@ -263,6 +263,100 @@ __device__ __forceinline__ V3 newton_step(const float acc[9], float4 uu, float4 
               (float)((C02 * f0 + C12 * f1 + C22 * f2) * iD));
 }
 
+// ------------------------------------------------------------------------ colour kernels
+// Per-vertex epilogue. mode 0: VBD solve; mode 1: VBD residual (writes |r| reductions);
+// mode 2: explicit force (kernel_fem_eval_force, GPU_FEM_Explicit.cu:5-64).
+__device__ __forceinline__ void vertex_epilogue(const SceneDev& S, int vid, const float acc[9], int mode, const StepParams& P,
+                                                double* red) {
+    const float4 uu = S.u[vid], ul = S.u_last[vid], yy = S.y[vid];
+    if (mode == 0) {
+        const V3 d = newton_step(acc, uu, ul, yy, S.damping, P.inv_dt, S.precision);
+        const float4 un = make_float4(uu.x + d.x, uu.y + d.y, uu.z + d.z, uu.w);
+        if (P.in_place) S.u[vid] = un; else S.u_new[vid] = un;
+    } else if (mode == 1) {
+        // kernel_vbd_compute_residual (GPU_VBD_FEM.cu:482-546)
+        const float kd = S.damping * P.inv_dt, mh2 = yy.w * P.inv_dt * P.inv_dt;
+        const float dx = uu.x - ul.x, dy = uu.y - ul.y, dz = uu.z - ul.z;
+        const double r0 = acc[0] - kd * (acc[3] * dx + acc[4] * dy + acc[5] * dz) - mh2 * (uu.x - yy.x);
+        const double r1 = acc[1] - kd * (acc[4] * dx + acc[6] * dy + acc[7] * dz) - mh2 * (uu.y - yy.y);
+        const double r2 = acc[2] - kd * (acc[5] * dx + acc[7] * dy + acc[8] * dz) - mh2 * (uu.z - yy.z);
+        const double nr = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
+        if (!isfinite(nr)) atomicOr(P.error, 2);
+        else {
+            atomicAdd(red, nr);
+            unsigned long long* mx = reinterpret_cast<unsigned long long*>(red + 1);
+            atomicMax(mx, (unsigned long long)__double_as_longlong(nr));
+        }
+    } else {
+        // f = sum(-P g V) - k_d H v, written to u_new (the force buffer of the explicit solver)
+        const float4 vv = S.v[vid];
+        const float kd = S.damping;
+        float4 f;
+        f.x = acc[0] - kd * (acc[3] * vv.x + acc[4] * vv.y + acc[5] * vv.z);
+        f.y = acc[1] - kd * (acc[4] * vv.x + acc[6] * vv.y + acc[7] * vv.z);
+        f.z = acc[2] - kd * (acc[5] * vv.x + acc[7] * vv.y + acc[8] * vv.z);
+        f.w = 0.f;
+        S.u_new[vid] = f;
+    }
+}
+
+// Packed mapping: one lane per (vertex, owner) pair.  The host packs whole vertices of one
+// colour into warp items (at most 32 pairs each), so lanes are busy whatever the valences;
+// each vertex's terms are then summed with a segmented shuffle reduction into its first
+// lane, which runs the epilogue.
+template <int E, int MAT>
+__global__ void __launch_bounds__(kBlock) k_vertex_packed(const SceneDev* __restrict__ scenes,
+                                                          const VWork* __restrict__ work, int n_work, int mode,
+                                                          StepParams P, double* red) {
+    constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ;
+    __shared__ __align__(128) float s_dN[((NQ * NE * 3 + 3) / 4) * 4];
+    __shared__ __align__(8) unsigned long long s_mbar;
+    stage_table(s_dN, gdN<E>(), NQ * NE * 3, &s_mbar, P.error);
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int wpb = kBlock / 32;
+    for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < n_work; w += gridDim.x * wpb) {
+        const VWork wk = work[w];
+        const SceneDev& S = scenes[wk.scene];
+        // pair offset of each slot start relative to the item (lane n_slots holds the end)
+        int start = 32;
+        if (lane <= wk.count) start = __ldg(S.own_off + wk.slot_begin + lane) - wk.pair_base;
+        const int n_pairs = __shfl_sync(full, start, wk.count);
+        const unsigned heads = __reduce_or_sync(full, (lane < wk.count) ? (1u << start) : 0u);
+        const unsigned upto = heads & ((2u << lane) - 1u);
+        const int seg = __popc(upto) - 1;
+        const int head = 31 - __clz(upto);
+        const unsigned above = heads & ~((2u << lane) - 1u);
+        const int seg_end = above ? __ffs(above) - 1 : n_pairs;
+        int vid = 0;
+        bool active = false;
+        if (lane < n_pairs) {
+            vid = __ldg(S.vids + wk.slot_begin + seg);
+            active = mode == 2 || S.mask[vid] != 0;
+        }
+        float acc[9], cmp[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) { acc[k] = 0.f; cmp[k] = 0.f; }
+        const bool mixed = S.precision != 0;
+        if (active) {
+            owner_terms<E, MAT>(S, __ldg(S.owners + wk.pair_base + lane), s_dN, mixed, acc, cmp);
+            if (mixed) {
+#pragma unroll
+                for (int k = 0; k < 9; ++k) acc[k] -= cmp[k];
+            }
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                const float o = __shfl_down_sync(full, acc[k], off);
+                if (lane + off < seg_end) acc[k] += o;
+            }
+        }
+        if (active && lane == head) vertex_epilogue(S, vid, acc, mode, P, red);
+    }
+}
+
 // ------------------------------------------------------------------------ colour kernel
 // mode 0: VBD solve; mode 1: VBD residual (writes |r| reductions); mode 2: explicit force.
 template <int E, int MAT>
@@ -304,38 +398,7 @@ __global__ void __launch_bounds__(kBlock) k_vertex(const SceneDev* __restrict__ 
 #pragma unroll
             for (int k = 0; k < 9; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], off);
         }
-        if (active && glane == 0) {
-            const float4 uu = S.u[vid], ul = S.u_last[vid], yy = S.y[vid];
-            if (mode == 0) {
-                const V3 d = newton_step(acc, uu, ul, yy, S.damping, P.inv_dt, S.precision);
-                const float4 un = make_float4(uu.x + d.x, uu.y + d.y, uu.z + d.z, uu.w);
-                if (P.in_place) S.u[vid] = un; else S.u_new[vid] = un;
-            } else if (mode == 1) {
-                // kernel_vbd_compute_residual (GPU_VBD_FEM.cu:482-546)
-                const float kd = S.damping * P.inv_dt, mh2 = yy.w * P.inv_dt * P.inv_dt;
-                const float dx = uu.x - ul.x, dy = uu.y - ul.y, dz = uu.z - ul.z;
-                const double r0 = acc[0] - kd * (acc[3] * dx + acc[4] * dy + acc[5] * dz) - mh2 * (uu.x - yy.x);
-                const double r1 = acc[1] - kd * (acc[4] * dx + acc[6] * dy + acc[7] * dz) - mh2 * (uu.y - yy.y);
-                const double r2 = acc[2] - kd * (acc[5] * dx + acc[7] * dy + acc[8] * dz) - mh2 * (uu.z - yy.z);
-                const double nr = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
-                if (!isfinite(nr)) atomicOr(P.error, 2);
-                else {
-                    atomicAdd(red, nr);
-                    unsigned long long* mx = reinterpret_cast<unsigned long long*>(red + 1);
-                    atomicMax(mx, (unsigned long long)__double_as_longlong(nr));
-                }
-            } else {
-                // kernel_fem_eval_force (GPU_FEM_Explicit.cu:5-64): f = sum(-P g V) - k_d H v
-                const float4 vv = S.v[vid];
-                const float kd = S.damping;
-                float4 f;
-                f.x = acc[0] - kd * (acc[3] * vv.x + acc[4] * vv.y + acc[5] * vv.z);
-                f.y = acc[1] - kd * (acc[4] * vv.x + acc[6] * vv.y + acc[7] * vv.z);
-                f.z = acc[2] - kd * (acc[5] * vv.x + acc[7] * vv.y + acc[8] * vv.z);
-                f.w = 0.f;
-                S.u_new[vid] = f;
-            }
-        }
+        if (active && glane == 0) vertex_epilogue(S, vid, acc, mode, P, red);
     }
 }
 
@@ -445,6 +508,34 @@ __global__ void k_constraints(const SceneDev* __restrict__ scenes, const NWork* 
         u.x = px - X.x; u.y = py - X.y; u.z = pz - X.z;
         S.u[k] = u;
     }
+}
+
+// Host-state staging of a batch: state[off_s + 3 i ...] = u_i then v_i (n*3 floats each).
+// dir 0: staging -> node arrays, dir 1: node arrays -> staging.
+__global__ void k_state(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work, const long long* __restrict__ soff,
+                        float* __restrict__ state, int dir) {
+    const NWork wk = work[blockIdx.x];
+    if (threadIdx.x >= wk.count) return;
+    const SceneDev& S = scenes[wk.scene];
+    const int i = wk.begin + threadIdx.x;
+    float* p = state + soff[wk.scene] + 3ll * i;
+    float* v = state + soff[wk.scene] + 3ll * S.n_nodes + 3ll * i;
+    if (dir == 0) {
+        float4 u = S.u[i];
+        u.x = p[0]; u.y = p[1]; u.z = p[2];
+        S.u[i] = u;
+        S.v[i] = make_float4(v[0], v[1], v[2], 0.f);
+    } else {
+        const float4 u = S.u[i], w = S.v[i];
+        p[0] = u.x; p[1] = u.y; p[2] = u.z;
+        v[0] = w.x; v[1] = w.y; v[2] = w.z;
+    }
+}
+
+void launch_state(const SceneDev* scenes, const NWork* work, int n_work, const long long* soff, float* state, int dir,
+                  cudaStream_t st) {
+    if (n_work <= 0) return;
+    k_state<<<n_work, kNodeChunk, 0, st>>>(scenes, work, soff, state, dir);
 }
 
 // Jacobi commit of a colour (kernel_copy_in_position, GPU_VBD_FEM.cu:402-413).
@@ -675,12 +766,31 @@ template <class K> int persistent_grid(K kernel, int n_work) {
     return n_work < g ? n_work : g;
 }
 
+// Persistent grid size (SMs x resident blocks) of each vertex-kernel instantiation,
+// computed once outside any stream capture by prepare_vertex.
+template <int E, int MAT, bool PACKED> int& grid_cap() {
+    static int cap = 0;
+    return cap;
+}
+
 template <int E, int MAT>
 void vertex_dispatch(const SceneDev* scenes, const VWork* work, int n_work, int tpv, int mode, const StepParams& P,
                      double* red, cudaStream_t st) {
-    static int grid_cap = 0;
-    if (!grid_cap) grid_cap = persistent_grid(k_vertex<E, MAT>, 1 << 30);
-    const int grid = n_work < grid_cap ? n_work : grid_cap;
+    if (mode < 0) {   // preparation call: fill the caches only
+        if (grid_cap<E, MAT, false>() <= 0) grid_cap<E, MAT, false>() = persistent_grid(k_vertex<E, MAT>, 1 << 30);
+        if (grid_cap<E, MAT, true>() <= 0) grid_cap<E, MAT, true>() = persistent_grid(k_vertex_packed<E, MAT>, 1 << 30);
+        return;
+    }
+    if (tpv == 0) {
+        int cap = grid_cap<E, MAT, true>();
+        if (cap <= 0) cap = 148 * 4;
+        const int blocks = (n_work + kBlock / 32 - 1) / (kBlock / 32);
+        k_vertex_packed<E, MAT><<<blocks < cap ? blocks : cap, kBlock, 0, st>>>(scenes, work, n_work, mode, P, red);
+        return;
+    }
+    int cap = grid_cap<E, MAT, false>();
+    if (cap <= 0) cap = 148 * 4;
+    const int grid = n_work < cap ? n_work : cap;
     k_vertex<E, MAT><<<grid, kBlock, 0, st>>>(scenes, work, n_work, tpv, mode, P, red);
 }
 
@@ -754,6 +864,11 @@ cudaError_t upload_shape_tables(int element, const float* dN, int n_floats) {
         default: return cudaErrorInvalidValue;
     }
     return e1 != cudaSuccess ? e1 : e2;
+}
+
+void prepare_vertex(int element, int material) {
+    StepParams P{};
+    launch_vertex(element, material, nullptr, nullptr, 1, 1, -1, P, nullptr, nullptr);
 }
 
 void launch_vertex(int element, int material, const SceneDev* scenes, const VWork* work, int n_work, int tpv, int mode,

@@ -7,6 +7,9 @@
 namespace octb {
 
 cudaError_t upload_shape_tables(int element, const float* dN, int n_floats);
+// Caches the persistent grid size of the vertex kernel for (element, material); call
+// outside stream capture.
+void prepare_vertex(int element, int material);
 // mode 0: VBD solve, 1: VBD residual (red[0] += |r|, red[1] = max |r|), 2: explicit force
 void launch_vertex(int element, int material, const SceneDev* scenes, const VWork* work, int n_work, int tpv, int mode,
                    const StepParams& P, double* red, cudaStream_t st);
@@ -24,6 +27,9 @@ void launch_xpbd(int element, int material, const SceneDev* scenes, const int* e
 void launch_energy(int element, int material, const SceneDev* scenes, int scene, int n_nodes, int n_elements, double* out,
                    int* error, cudaStream_t st);
 
+// Batch host-state staging: dir 0 scatters state into u/v, dir 1 gathers u/v into state.
+void launch_state(const SceneDev* scenes, const NWork* work, int n_work, const long long* soff, float* state, int dir,
+                  cudaStream_t st);
 // FP32 FMA microbenchmark: returns the number of FMAs issued by the launch.
 double launch_fma_peak(cudaStream_t st);
 // Algorithmic FP32 flops of one (owner, quadrature point) term of the VBD kernel.

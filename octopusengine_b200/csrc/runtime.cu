@@ -36,13 +36,17 @@ struct oct_ctx {
     float last_ms = 0.f;
     uint64_t launches = 0;
     bool tables[10] = {false};
-    std::mutex mu;   // guards the budget accounting and the shape-table upload
+    std::mutex mu;       // guards the budget accounting and the shape-table upload
+    std::mutex err_mu;   // guards err (scenes may be created from several host threads)
 };
 
 namespace {
 
 oct_status fail(oct_ctx* c, oct_status s, const std::string& msg) {
-    if (c) c->err = msg;
+    if (c) {
+        std::lock_guard<std::mutex> lock(c->err_mu);
+        c->err = msg;
+    }
     return s;
 }
 
@@ -89,6 +93,7 @@ struct oct_scene {
     bool in_place = true, box = false, has_v0 = false;
     std::mt19937 rng;
     std::vector<int32_t> colors, vids, color_off;   // colour-sorted slots
+    std::vector<int32_t> own_off;                    // owner CSR offsets in slot order (host copy)
     std::vector<float> masses, X;
     std::vector<int32_t> fixed;
     // device
@@ -138,6 +143,8 @@ struct oct_batch {
     float graph_dt = -1.f;
     int graph_pending = -1;
     std::vector<size_t> state_off;
+    long long* d_soff = nullptr;    // per-scene offsets into the staging buffer
+    float* d_state = nullptr;       // staging buffer, allocated on first host-state transfer
 };
 
 namespace {
@@ -154,10 +161,25 @@ oct_status ensure_tables(oct_ctx* c, int element) {
     return OCT_OK;
 }
 
-// Split [begin, end) slots into block-sized work items for one scene.
-void append_vwork(std::vector<VWork>& out, int scene, int begin, int end, int tpv) {
-    const int vpb = kBlockThreads / tpv;
-    for (int s = begin; s < end; s += vpb) out.push_back({scene, s, std::min(vpb, end - s), 0});
+// Split [begin, end) slots into work items for one scene: block-sized items of 128 / tpv
+// slots, or (tpv == 0) warp items packing whole vertices up to 32 (vertex, owner) pairs
+// and at most 31 slots.
+void append_vwork(std::vector<VWork>& out, int scene, int begin, int end, int tpv, const std::vector<int32_t>& own_off) {
+    if (tpv > 0) {
+        const int vpb = kBlockThreads / tpv;
+        for (int s = begin; s < end; s += vpb) out.push_back({scene, s, std::min(vpb, end - s), 0});
+        return;
+    }
+    int s = begin;
+    while (s < end) {
+        int pairs = 0, n = 0;
+        while (s + n < end && n < 31 && pairs + (own_off[s + n + 1] - own_off[s + n]) <= 32) {
+            pairs += own_off[s + n + 1] - own_off[s + n];
+            ++n;
+        }
+        out.push_back({scene, s, n, own_off[s]});
+        s += n;
+    }
 }
 void append_nwork(std::vector<NWork>& out, int scene, int n) {
     for (int s = 0; s < n; s += kNodeChunk) out.push_back({scene, s, std::min(kNodeChunk, n - s), 0});
@@ -208,6 +230,10 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     if ((int64_t)E >= (1ll << (31 - kOwnerShift))) return fail(c, OCT_EINVAL, "too many elements for one scene");
     oct_status st = ensure_tables(c, d->element);
     if (st) return st;
+    {
+        std::lock_guard<std::mutex> lock(c->mu);
+        prepare_vertex(d->element, d->material);
+    }
     s->iterations = std::max(1, d->iterations);
     s->rho = d->rho;
     s->order_mode = d->order_mode;
@@ -216,9 +242,9 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     s->global_damping = d->global_damping;
     s->box = d->box_limit != 0;
     s->has_v0 = d->initial_velocity != nullptr;
-    s->tpv = d->threads_per_vertex > 0 ? d->threads_per_vertex : default_tpv(d->element);
-    if (s->tpv != 1 && s->tpv != 2 && s->tpv != 4 && s->tpv != 8 && s->tpv != 16 && s->tpv != 32)
-        return fail(c, OCT_EINVAL, "threads_per_vertex must be a power of two <= 32");
+    s->tpv = d->threads_per_vertex;
+    if (s->tpv != 0 && s->tpv != 1 && s->tpv != 2 && s->tpv != 4 && s->tpv != 8 && s->tpv != 16 && s->tpv != 32)
+        return fail(c, OCT_EINVAL, "threads_per_vertex must be 0 (packed) or a power of two <= 32");
     s->X.assign(d->positions, d->positions + 3 * (size_t)N);
 
     // masses (Cuda_FEM_Dynamic::get_fem_masses)
@@ -336,11 +362,17 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
         for (int j = 0; j < NE; ++j) vown[vf[d->topology[(size_t)e * NE + j]]++] = (e << kOwnerShift) | j;
     std::vector<int32_t> own_off(N + 1, 0), owners;
     owners.reserve(vown.size());
+    int max_valence = 0;
     for (int sl = 0; sl < N; ++sl) {
         const int v = slot_vids[sl];
         owners.insert(owners.end(), vown.begin() + voff[v], vown.begin() + voff[v + 1]);
         own_off[sl + 1] = (int32_t)owners.size();
+        max_valence = std::max(max_valence, own_off[sl + 1] - own_off[sl]);
     }
+    // default mapping: one lane per (vertex, owner) pair packed into warps; vertices with
+    // more than 32 owners fall back to a fixed lane group per vertex
+    if (s->tpv == 0 && max_valence > 32) s->tpv = max_valence > 64 ? 32 : default_tpv(d->element);
+    s->own_off = own_off;
 
     // device state
     std::vector<float4> X4(N), y4(N), zero4(N, make_float4(0, 0, 0, 0)), v4(N, make_float4(0, 0, 0, 0));
@@ -390,7 +422,7 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     std::vector<VWork> vw;
     s->vwork_off.assign(1, 0);
     for (int k = 0; k + 1 < (int)s->color_off.size(); ++k) {
-        append_vwork(vw, 0, s->color_off[k], s->color_off[k + 1], s->tpv);
+        append_vwork(vw, 0, s->color_off[k], s->color_off[k + 1], s->tpv, s->own_off);
         s->vwork_off.push_back((int)vw.size());
     }
     std::vector<NWork> nw, fw;
@@ -560,6 +592,19 @@ oct_status oct_ctx_memory(oct_ctx* c, size_t* used, size_t* budget) {
     if (!c) return OCT_EINVAL;
     if (used) *used = c->used;
     if (budget) *budget = c->budget;
+    return OCT_OK;
+}
+
+oct_status oct_scene_footprint(const oct_scene_desc* d, size_t* bytes) {
+    if (!d || !bytes) return OCT_EINVAL;
+    const int ne = element_nodes(d->element), nq = element_quadrature(d->element);
+    if (ne < 0 || d->n_nodes <= 0 || d->n_elements <= 0) return OCT_EINVAL;
+    const size_t N = d->n_nodes, E = d->n_elements;
+    size_t b = N * (6 * sizeof(float4) + 3 * sizeof(int)) + (d->rho > 0.f ? 2 * N * sizeof(float4) : 0);
+    b += E * ne * sizeof(int) * 2 + E * nq * 3 * sizeof(float4);   // topology, owners, quadrature records
+    b += (N / 16 + 64) * sizeof(VWork) + (N / 256 + 8) * 2 * sizeof(NWork) + (size_t)std::max(d->n_fixed, 0) * sizeof(int);
+    b += 4096;   // descriptors and reduction scratch
+    *bytes = b;
     return OCT_OK;
 }
 
@@ -765,7 +810,7 @@ oct_status oct_batch_create(oct_ctx* c, oct_scene* const* scenes, int n, oct_bat
         }
         auto& cw = gwork[it->second];
         if ((int)cw.size() < s->n_colors) cw.resize(s->n_colors);
-        for (int k = 0; k < s->n_colors; ++k) append_vwork(cw[k], i, s->color_off[k], s->color_off[k + 1], s->tpv);
+        for (int k = 0; k < s->n_colors; ++k) append_vwork(cw[k], i, s->color_off[k], s->color_off[k + 1], s->tpv, s->own_off);
         append_nwork(nw, i, s->n_nodes);
         std::vector<NWork> f1;
         append_nwork(f1, i, s->n_fixed);
@@ -792,6 +837,8 @@ oct_status oct_batch_create(oct_ctx* c, oct_scene* const* scenes, int n, oct_bat
         b->mem.release();
         return st;
     }
+    std::vector<long long> soff(b->state_off.begin(), b->state_off.end());
+    if ((st = upload(c, b->mem, b->d_soff, soff))) { b->mem.release(); return st; }
     b->n_nwork = (int)nw.size();
     b->n_fwork = (int)fw.size();
     b->n_bwork = (int)bw.size();
@@ -941,35 +988,27 @@ oct_status oct_batch_state_size(oct_batch* b, size_t* n) {
 }
 
 // Host <-> device state transfer of a batch: per scene n*3 displacements (p - X) then n*3
-// velocities, each moved with one strided copy into the float4 node arrays
-// (cudaMemcpy2DAsync: 12 of every 16 bytes).
+// velocities.  One contiguous copy to/from a device staging buffer and one kernel that
+// scatters/gathers the float4 node arrays.
 oct_status oct_batch_set_state(oct_batch* b, const float* host) {
     if (!b || !host) return OCT_EINVAL;
     oct_ctx* c = b->ctx;
-    for (size_t i = 0; i < b->scenes.size(); ++i) {
-        oct_scene* s = b->scenes[i];
-        const float* p = host + b->state_off[i];
-        const float* v = p + 3 * (size_t)s->n_nodes;
-        OCT_CUDA(c, cudaMemcpy2DAsync(s->h.u, sizeof(float4), p, 3 * sizeof(float), 3 * sizeof(float), s->n_nodes,
-                                      cudaMemcpyHostToDevice, c->stream));
-        OCT_CUDA(c, cudaMemcpy2DAsync(s->h.v, sizeof(float4), v, 3 * sizeof(float), 3 * sizeof(float), s->n_nodes,
-                                      cudaMemcpyHostToDevice, c->stream));
-    }
+    const size_t n = b->state_off.back();
+    if (!b->d_state) { oct_status st = b->mem.alloc(b->d_state, n); if (st) return st; }
+    OCT_CUDA(c, cudaMemcpyAsync(b->d_state, host, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    launch_state(b->d_scenes, b->d_nwork, b->n_nwork, b->d_soff, b->d_state, 0, c->stream);
+    c->launches++;
     return OCT_OK;
 }
 
 oct_status oct_batch_get_state(oct_batch* b, float* host) {
     if (!b || !host) return OCT_EINVAL;
     oct_ctx* c = b->ctx;
-    for (size_t i = 0; i < b->scenes.size(); ++i) {
-        oct_scene* s = b->scenes[i];
-        float* p = host + b->state_off[i];
-        float* v = p + 3 * (size_t)s->n_nodes;
-        OCT_CUDA(c, cudaMemcpy2DAsync(p, 3 * sizeof(float), s->h.u, sizeof(float4), 3 * sizeof(float), s->n_nodes,
-                                      cudaMemcpyDeviceToHost, c->stream));
-        OCT_CUDA(c, cudaMemcpy2DAsync(v, 3 * sizeof(float), s->h.v, sizeof(float4), 3 * sizeof(float), s->n_nodes,
-                                      cudaMemcpyDeviceToHost, c->stream));
-    }
+    const size_t n = b->state_off.back();
+    if (!b->d_state) { oct_status st = b->mem.alloc(b->d_state, n); if (st) return st; }
+    launch_state(b->d_scenes, b->d_nwork, b->n_nwork, b->d_soff, b->d_state, 1, c->stream);
+    c->launches++;
+    OCT_CUDA(c, cudaMemcpyAsync(host, b->d_state, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     OCT_CUDA(c, cudaStreamSynchronize(c->stream));
     return OCT_OK;
 }

@@ -1,0 +1,43 @@
+"""The reference-shaped C++ adapters (include/octopus_b200.hpp: GPU_ParticleSystem, GPU_VBD,
+GPU_VBD_FEM, GPU_Fix_Constraint, compute_fem_mass) drive the same C ABI and reproduce the
+Python-path and oracle results on config 1."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from scenes import rel_err
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _compile(tmp_path):
+    exe = str(tmp_path / "adapter_demo")
+    subprocess.check_call(["g++", "-std=c++17", "-O2", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "cpp", "adapter_demo.cpp"),
+                           "-L", os.path.join(ROOT, "octopusengine_b200"), "-loctb",
+                           "-Wl,-rpath," + os.path.join(ROOT, "octopusengine_b200"), "-o", exe])
+    return exe
+
+
+def test_adapter_compiles(built, tmp_path):
+    assert os.path.exists(_compile(tmp_path))
+
+
+@pytest.mark.gpu
+def test_adapter_matches_oracle(built, tmp_path):
+    exe = _compile(tmp_path)
+    out = subprocess.check_output([exe, "5"], text=True)
+    p = np.array([[float(v) for v in ln.split()] for ln in out.strip().split("\n")])
+    X, T = O.beam_mesh(O.TETRA, (8, 2, 2), (1.0, 0.25, 0.25))
+    m = O.masses(O.TETRA, X, T, 1000.0, 1)
+    fixed = O.fixed_by_plane(X, (0.01, 0, 0), (-1, 0, 0))
+    c, n = O.colour(O.TETRA, T, len(X), 0)
+    s = O.Scene(O.TETRA, X, T, m, young=1e5, poisson=0.45, fixed=fixed, iterations=20, colors=c, n_colors=n,
+                in_place=True)
+    ref = O.Solver("vbd", s, fp64=True)
+    for _ in range(5):
+        ref.step(0.01, 1)
+    assert rel_err(p, ref.get(0)) < 1e-5

@@ -91,7 +91,7 @@ def test_initial_velocity_and_chebyshev(ctx):
     assert rel_err(s.get_position(), o64.get(0)) < 1e-5
 
 
-@pytest.mark.parametrize("tpv", [1, 2, 4, 16, 32])
+@pytest.mark.parametrize("tpv", [0, 1, 2, 4, 16, 32])
 def test_threads_per_vertex_do_not_change_results(ctx, tpv):
     s, o32, o64, mesh = pair(ctx, O.TETRA, cells=(6, 2, 2), iterations=5, tpv=tpv)
     s.step(0.01, 1)
@@ -120,3 +120,38 @@ def test_residual_and_energy_are_finite_and_decrease(ctx):
     ro = o64.residual(0.01)
     assert np.isfinite(r1).all()
     assert abs(r1[0] - ro[0]) / max(ro[0], 1e-30) < 1e-3
+
+
+def _star_mesh(n_fan=40):
+    """A fan of n_fan tetrahedra around one apex: the apex has n_fan owners (more than a
+    warp), which exercises the fixed-lane-group fallback of the packed mapping."""
+    ang = np.linspace(0, 2 * np.pi, n_fan, endpoint=False)
+    ring = np.stack([np.cos(ang), np.sin(ang), np.zeros_like(ang)], 1) * 0.2
+    X = np.concatenate([[[0, 0, 0.1], [0, 0, -0.1]], ring + [0, 0, 0]]).astype(np.float32)
+    T = []
+    for k in range(n_fan):
+        a, b = 2 + k, 2 + (k + 1) % n_fan
+        T.append([0, 1, a, b])
+    T = np.array(T, np.int32)
+    # orient positively
+    for t in T:
+        p = X[t]
+        if np.linalg.det(np.stack([p[1] - p[0], p[2] - p[0], p[3] - p[0]], 1)) < 0:
+            t[2], t[3] = t[3], t[2]
+    return X, T
+
+
+def test_high_valence_fallback(ctx):
+    import octopusengine_b200 as ob
+    X, T = _star_mesh(40)
+    m = O.masses(O.TETRA, X, T, 1000.0, 1)
+    fixed = np.array([1], np.int32)
+    s = ob.Scene(ctx, O.TETRA, X, T, masses=m, young=1e5, poisson=0.3, fixed_ids=fixed, iterations=4,
+                 gravity=(0.0, 0.0, -9.81))
+    c, n = O.colour(O.TETRA, T, len(X), 0)
+    ref = O.Solver("vbd", O.Scene(O.TETRA, X, T, m, young=1e5, poisson=0.3, fixed=fixed, iterations=4, colors=c,
+                                  n_colors=n, in_place=True), fp64=True)
+    for _ in range(3):
+        s.step(0.01, 1)
+        ref.step(0.01, 1)
+    assert rel_err(s.get_position(), ref.get(0)) < 1e-5
