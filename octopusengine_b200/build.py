@@ -25,12 +25,26 @@ EXTRA = os.environ.get("OCTB_NVCC_FLAGS", "").split()
 
 
 def _sources():
-    return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp")))
+    srcs = glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cpp"))
+    return sorted(s for s in srcs if not s.endswith("gen_tables.cpp"))
+
+
+def _gen_tables():
+    """Compiles and runs gen_tables.cpp (host only) to write csrc/shape_tables.inc."""
+    out = os.path.join(CSRC, "shape_tables.inc")
+    deps = [os.path.join(CSRC, f) for f in ("gen_tables.cpp", "shape.cpp", "host.hpp")]
+    if os.path.exists(out) and os.path.getmtime(out) >= max(os.path.getmtime(d) for d in deps):
+        return
+    exe = os.path.join(BUILD, "gen_tables")
+    subprocess.check_call([os.environ.get("CXX", "g++"), "-O1", "-std=c++17", "-I", CSRC, deps[0], deps[1], "-o", exe])
+    txt = subprocess.check_output([exe], text=True)
+    with open(out, "w") as f:
+        f.write(txt)
 
 
 def _headers():
     return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) + \
-        glob.glob(os.path.join(ROOT, "include", "*.h"))
+        glob.glob(os.path.join(CSRC, "*.inc")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
 
 
 def _compile(src, verbose=False):
@@ -52,6 +66,7 @@ def _compile(src, verbose=False):
 
 def build(verbose=False, jobs=None):
     os.makedirs(BUILD, exist_ok=True)
+    _gen_tables()
     srcs = _sources()
     with cf.ThreadPoolExecutor(max_workers=jobs or min(8, len(srcs))) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), srcs))

@@ -8,8 +8,12 @@
 // positions cause in FP32 (F of the rest state is exactly I).
 //
 // Element data: topology E*NE ints, and per (element, quadrature point) a 48-byte record
-// of three float4: JX_inv (column-major 9 floats), V = |det J| w_q, lambda, mu.  The
-// inverse reference Jacobians are computed in FP64 on the host and rounded once.
+// of three float4: JX_inv (column-major 9 floats), |det J|, lambda, mu (the quadrature
+// volume is |det J| w_q with the compile-time weight w_q).  When every element's map is
+// affine (straight-sided tetrahedra, parallelepiped hexahedra: all beam meshes) J does not
+// vary over the quadrature points and one record per element is stored (eq_stride = 1
+// instead of NQ), which divides the per-visit element bytes by NQ.  The inverse reference
+// Jacobians are computed in FP64 on the host and rounded once.
 //
 // Colour-sorted vertex slots: vids[slot] is the node solved in that slot; slots of colour
 // c are [color_off[c], color_off[c+1]) in ascending node id (GPU_VBD_FEM::create_buffers,
@@ -42,6 +46,7 @@ struct SceneDev {
     const int* owners;  // packed (eid << 5) | r
     const int* fixed;   // n_fixed node ids
     int n_nodes, n_elements, n_fixed, element;
+    int eq_stride;                     // records per element: NQ, or 1 for affine elements
     float damping;      // k_d
     float gx, gy, gz;
     float comx, comy, comz;            // fixed-set centre of mass (float, as the reference)

@@ -30,6 +30,7 @@
 
 #include "device.cuh"
 #include "kernels.cuh"
+#include "shape_tables.inc"
 
 namespace octb {
 
@@ -65,6 +66,19 @@ template <> __device__ __forceinline__ const float* gdN<6>() { return g_dN6; }
 template <> __device__ __forceinline__ const float* gdN<7>() { return g_dN7; }
 template <> __device__ __forceinline__ const float* gdN<8>() { return g_dN8; }
 template <> __device__ __forceinline__ const float* gdN<9>() { return g_dN9; }
+
+// Reference-element derivative dN_qi[k] and quadrature weight w_q.  For every element but
+// Hexa_27 the loops that read them are fully unrolled, so they are compile-time constants
+// (exact zeros drop out of the FMAs); Hexa_27's 27 x 27 table is read from constant memory.
+template <int E> __device__ __forceinline__ float dn(int q, int i, int k) {
+    if constexpr (E == 9) return c_dN9[(q * 27 + i) * 3 + k];
+    else return ShapeConst<E>::dN((q * ElemT<E>::NE + i) * 3 + k);
+}
+__constant__ float c_w9[27];
+template <int E> __device__ __forceinline__ float wq(int q) {
+    if constexpr (E == 9) return c_w9[q];
+    else return ShapeConst<E>::w(q);
+}
 
 constexpr int kBlock = 128;
 constexpr long kSpinLimit = 1L << 22;
@@ -182,31 +196,32 @@ __device__ __forceinline__ void owner_terms(const SceneDev& S, int packed, const
         const float4 t = __ldg(&S.u[__ldg(tp + i)]);
         ux[i] = t.x; uy[i] = t.y; uz[i] = t.z;
     }
-    const float4* __restrict__ rec = S.eq + (size_t)eid * NQ * 3;
-    const float* cd = cdN<E>();
+    const bool affine = S.eq_stride == 1;
+    const float4* __restrict__ rec = S.eq + (size_t)eid * S.eq_stride * 3;
+    float4 A = __ldg(rec), B = __ldg(rec + 1), C = __ldg(rec + 2);
 #pragma unroll (NQ <= 11 ? NQ : 1)
     for (int q = 0; q < NQ; ++q) {
-        const float4 A = __ldg(rec + 3 * q), B = __ldg(rec + 3 * q + 1), C = __ldg(rec + 3 * q + 2);
+        if (!affine && q > 0) { A = __ldg(rec + 3 * q); B = __ldg(rec + 3 * q + 1); C = __ldg(rec + 3 * q + 2); }
         // Jx columns: Jk = sum_i u_i dN_qi[k]
         V3 J0 = mk(0, 0, 0), J1 = mk(0, 0, 0), J2 = mk(0, 0, 0);
 #pragma unroll
         for (int i = 0; i < NE; ++i) {
-            const float d0 = cd[(q * NE + i) * 3], d1 = cd[(q * NE + i) * 3 + 1], d2 = cd[(q * NE + i) * 3 + 2];
+            const float d0 = dn<E>(q, i, 0), d1 = dn<E>(q, i, 1), d2 = dn<E>(q, i, 2);
             J0.x = fmaf(ux[i], d0, J0.x); J0.y = fmaf(uy[i], d0, J0.y); J0.z = fmaf(uz[i], d0, J0.z);
             J1.x = fmaf(ux[i], d1, J1.x); J1.y = fmaf(uy[i], d1, J1.y); J1.z = fmaf(uz[i], d1, J1.z);
             J2.x = fmaf(ux[i], d2, J2.x); J2.y = fmaf(uy[i], d2, J2.y); J2.z = fmaf(uz[i], d2, J2.z);
         }
         // JX_inv columns m_b (m_b[k] = row k, column b)
         const V3 m0 = mk(A.x, A.y, A.z), m1 = mk(A.w, B.x, B.y), m2 = mk(B.z, B.w, C.x);
-        const float V = C.y, lam = C.z, mu = C.w;
+        const float V = C.y * wq<E>(q), lam = C.z, mu = C.w;
         // F_b = e_b + sum_k J_k m_b[k]
         V3 F0 = J0 * m0.x + J1 * m0.y + J2 * m0.z;
         V3 F1 = J0 * m1.x + J1 * m1.y + J2 * m1.z;
         V3 F2 = J0 * m2.x + J1 * m2.y + J2 * m2.z;
         F0.x += 1.f; F1.y += 1.f; F2.z += 1.f;
         const float* dr = s_dN + (q * NE + r) * 3;
-        const V3 dn = mk(dr[0], dr[1], dr[2]);
-        const V3 g = mk(dot(m0, dn), dot(m1, dn), dot(m2, dn));
+        const V3 dnr = mk(dr[0], dr[1], dr[2]);
+        const V3 g = mk(dot(m0, dnr), dot(m1, dnr), dot(m2, dnr));
         float t[9];
         material_terms<MAT>(F0, F1, F2, g, lam, mu, V, t);
         if (mixed) {
@@ -611,7 +626,8 @@ __global__ void __launch_bounds__(kBlock) k_xpbd(const SceneDev* __restrict__ sc
     const SceneDev& S = scenes[scene];
     const int eid = elems[begin + t];
     const int* tp = S.topo + (size_t)eid * NE;
-    const float4* rec = S.eq + (size_t)eid * NQ * 3;
+    const float4* rec = S.eq + (size_t)eid * S.eq_stride * 3;
+    const int qs = S.eq_stride == 1 ? 0 : 1;
     const float* cd = cdN<E>();
     const float dt2 = P.dt * P.dt;
     for (int m = 0; m < 2; ++m) {
@@ -623,7 +639,7 @@ __global__ void __launch_bounds__(kBlock) k_xpbd(const SceneDev* __restrict__ sc
         }
         float C = 0.f, lam = 0.f, mu = 0.f;
         for (int q = 0; q < NQ; ++q) {
-            const float4 A = rec[3 * q], B = rec[3 * q + 1], Cr = rec[3 * q + 2];
+            const float4 A = rec[3 * q * qs], B = rec[3 * q * qs + 1], Cr = rec[3 * q * qs + 2];
             V3 J0 = mk(0, 0, 0), J1 = mk(0, 0, 0), J2 = mk(0, 0, 0);
 #pragma unroll
             for (int i = 0; i < NE; ++i) {
@@ -631,7 +647,7 @@ __global__ void __launch_bounds__(kBlock) k_xpbd(const SceneDev* __restrict__ sc
                 J0 = J0 + mk(ux[i], uy[i], uz[i]) * d0; J1 = J1 + mk(ux[i], uy[i], uz[i]) * d1; J2 = J2 + mk(ux[i], uy[i], uz[i]) * d2;
             }
             const V3 m0 = mk(A.x, A.y, A.z), m1 = mk(A.w, B.x, B.y), m2 = mk(B.z, B.w, Cr.x);
-            const float V = Cr.y;
+            const float V = Cr.y * wq<E>(q);
             lam = Cr.z; mu = Cr.w;
             V3 F0 = J0 * m0.x + J1 * m0.y + J2 * m0.z, F1 = J0 * m1.x + J1 * m1.y + J2 * m1.z, F2 = J0 * m2.x + J1 * m2.y + J2 * m2.z;
             F0.x += 1.f; F1.y += 1.f; F2.z += 1.f;
@@ -686,7 +702,8 @@ __global__ void k_energy_elements(const SceneDev* __restrict__ scenes, int scene
         const int* tp = S.topo + (size_t)eid * NE;
         const float* cd = cdN<E>();
         for (int q = 0; q < NQ; ++q) {
-            const float4 A = S.eq[((size_t)eid * NQ + q) * 3], B = S.eq[((size_t)eid * NQ + q) * 3 + 1], C = S.eq[((size_t)eid * NQ + q) * 3 + 2];
+            const size_t ri = ((size_t)eid * S.eq_stride + (S.eq_stride == 1 ? 0 : q)) * 3;
+            const float4 A = S.eq[ri], B = S.eq[ri + 1], C = S.eq[ri + 2];
             double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};   // J[col][row]
             for (int i = 0; i < NE; ++i) {
                 const float4 u = S.u[tp[i]];
@@ -699,7 +716,7 @@ __global__ void k_energy_elements(const SceneDev* __restrict__ scenes, int scene
             double F[3][3];   // F[col][row]
             for (int b = 0; b < 3; ++b)
                 for (int r = 0; r < 3; ++r) F[b][r] = (b == r ? 1.0 : 0.0) + J[0][r] * m[b][0] + J[1][r] * m[b][1] + J[2][r] * m[b][2];
-            const double lam = C.z, mu = C.w, V = C.y;
+            const double lam = C.z, mu = C.w, V = (double)C.y * (double)wq<E>(q);
             double psi;
             if (material == 2 || material == 3) {
                 const double det = F[0][0] * (F[1][1] * F[2][2] - F[2][1] * F[1][2]) - F[1][0] * (F[0][1] * F[2][2] - F[2][1] * F[0][2]) +
@@ -860,7 +877,15 @@ cudaError_t upload_shape_tables(int element, const float* dN, int n_floats) {
         case 6: e1 = cudaMemcpyToSymbol(c_dN6, dN, n_floats * 4); e2 = cudaMemcpyToSymbol(g_dN6, dN, n_floats * 4); break;
         case 7: e1 = cudaMemcpyToSymbol(c_dN7, dN, n_floats * 4); e2 = cudaMemcpyToSymbol(g_dN7, dN, n_floats * 4); break;
         case 8: e1 = cudaMemcpyToSymbol(c_dN8, dN, n_floats * 4); e2 = cudaMemcpyToSymbol(g_dN8, dN, n_floats * 4); break;
-        case 9: e1 = cudaMemcpyToSymbol(c_dN9, dN, n_floats * 4); e2 = cudaMemcpyToSymbol(g_dN9, dN, n_floats * 4); break;
+        case 9:
+            e1 = cudaMemcpyToSymbol(c_dN9, dN, n_floats * 4);
+            e2 = cudaMemcpyToSymbol(g_dN9, dN, n_floats * 4);
+            if (e1 == cudaSuccess) {
+                float w9[27];
+                for (int q = 0; q < 27; ++q) w9[q] = ShapeConst<9>::w(q);
+                e1 = cudaMemcpyToSymbol(c_w9, w9, sizeof(w9));
+            }
+            break;
         default: return cudaErrorInvalidValue;
     }
     return e1 != cudaSuccess ? e1 : e2;

@@ -299,13 +299,30 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
             I[0][2] = (J[0][1] * J[1][2] - J[1][1] * J[0][2]) * id;
             I[1][2] = -(J[0][0] * J[1][2] - J[1][0] * J[0][2]) * id;
             I[2][2] = (J[0][0] * J[1][1] - J[1][0] * J[0][1]) * id;
-            const float V = (float)(std::fabs(det) * sh.w[q]);
             float4* r = &eq[((size_t)e * NQ + q) * 3];
             r[0] = make_float4((float)I[0][0], (float)I[0][1], (float)I[0][2], (float)I[1][0]);
             r[1] = make_float4((float)I[1][1], (float)I[1][2], (float)I[2][0], (float)I[2][1]);
-            r[2] = make_float4((float)I[2][2], V, lam, mu);
+            r[2] = make_float4((float)I[2][2], (float)std::fabs(det), lam, mu);
         }
     }
+    // affine element maps (J the same at every quadrature point up to rounding, 1e-6
+    // relative): one record per element
+    bool affine = NQ > 1;
+    for (size_t e = 0; e < (size_t)E && affine; ++e) {
+        const float* r0 = reinterpret_cast<const float*>(&eq[e * NQ * 3]);
+        float scale = 0.f;
+        for (int k = 0; k < 9; ++k) scale = std::max(scale, std::fabs(r0[k]));
+        for (int q = 1; q < NQ && affine; ++q) {
+            const float* rq = reinterpret_cast<const float*>(&eq[(e * NQ + q) * 3]);
+            for (int k = 0; k < 9; ++k) affine = affine && std::fabs(rq[k] - r0[k]) <= 1e-6f * scale;
+            affine = affine && std::fabs(rq[9] - r0[9]) <= 1e-6f * std::fabs(r0[9]);
+        }
+    }
+    if (affine) {
+        for (size_t e = 1; e < (size_t)E; ++e) std::memmove(&eq[e * 3], &eq[e * NQ * 3], 3 * sizeof(float4));
+        eq.resize((size_t)E * 3);
+    }
+    s->h.eq_stride = affine || NQ == 1 ? 1 : NQ;
 
     // colouring and slot order
     std::vector<int32_t> slot_vids;
