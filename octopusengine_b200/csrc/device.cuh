@@ -47,6 +47,7 @@ struct SceneDev {
     const int* fixed;   // n_fixed node ids
     int n_nodes, n_elements, n_fixed, element;
     int eq_stride;                     // records per element: NQ, or 1 for affine elements
+    const float4* ent;                 // owner entries in slot order (EntryLayout), or null
     float damping;      // k_d
     float gx, gy, gz;
     float comx, comy, comz;            // fixed-set centre of mass (float, as the reference)
@@ -66,6 +67,18 @@ struct VWork {
     int slot_begin;
     int count;
     int pair_base;
+    unsigned heads;   // packed items: bit p set when pair p starts a new vertex
+    int n_pairs;      // packed items: number of (vertex, owner) pairs
+    int pad0, pad1;
+};
+
+// Owner entries (packed mapping): one record per (vertex, owner) pair in slot order,
+// contiguous per warp item so a single bulk copy stages a whole item in shared memory:
+// the owner element's NE node ids, the vertex's local index r, the element id, and (affine
+// scenes) the element's 12-float quadrature record; padded to a multiple of 4 words.
+template <int NE> struct EntryLayout {
+    static constexpr int kIds = 0, kR = NE, kEid = NE + 1, kRec = NE + 2;
+    static constexpr int kWords = ((NE + 2 + 12) + 3) / 4 * 4;
 };
 
 // One unit of node-parallel work (predictor, velocity update, Chebyshev).

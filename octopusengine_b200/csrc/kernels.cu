@@ -115,6 +115,33 @@ __device__ __forceinline__ void stage_table(float* s_dst, const float* g_src, in
     __syncthreads();
 }
 
+// ------------------------------------------------------------------------ L2 policies
+// Node displacements are gathered many times per sweep (every element around a node) and,
+// for a whole batch, fit in L2; the per-visit element stream (owners, topology, quadrature
+// records) is read once per visit.  Loads carry L2 eviction priorities accordingly:
+// gathers evict_last, streams evict_first (createpolicy + ld.global.nc.L2::cache_hint).
+__device__ __forceinline__ unsigned long long policy_keep() {
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ unsigned long long policy_stream() {
+    unsigned long long p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ float4 ld_hint(const float4* a, unsigned long long pol) {
+    float4 v;
+    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_hint(const int* a, unsigned long long pol) {
+    int v;
+    asm("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+    return v;
+}
+
 // ------------------------------------------------------------------------ helpers
 struct V3 { float x, y, z; };
 __device__ __forceinline__ V3 mk(float a, float b, float c) { return {a, b, c}; }
@@ -183,25 +210,18 @@ __device__ __forceinline__ void material_terms(V3 F0, V3 F1, V3 F2, V3 g, float 
     }
 }
 
-// f and H contributions of one owner element (all its quadrature points) to node r.
+// f and H contributions of one owner element (all its quadrature points) to its node r,
+// given the element's node displacements and its first quadrature record (A, B, C); for
+// non-affine elements the later records are read from rec.
 template <int E, int MAT>
-__device__ __forceinline__ void owner_terms(const SceneDev& S, int packed, const float* __restrict__ s_dN, bool mixed,
-                                            float acc[9], float cmp[9]) {
+__device__ __forceinline__ void element_terms(const float* ux, const float* uy, const float* uz, int r, float4 A, float4 B,
+                                              float4 C, const float4* __restrict__ rec, bool affine,
+                                              const float* __restrict__ s_dN, bool mixed, float acc[9], float cmp[9],
+                                              unsigned long long stream) {
     constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ;
-    const int eid = packed >> kOwnerShift, r = packed & ((1 << kOwnerShift) - 1);
-    const int* __restrict__ tp = S.topo + (size_t)eid * NE;
-    float ux[NE], uy[NE], uz[NE];
-#pragma unroll
-    for (int i = 0; i < NE; ++i) {
-        const float4 t = __ldg(&S.u[__ldg(tp + i)]);
-        ux[i] = t.x; uy[i] = t.y; uz[i] = t.z;
-    }
-    const bool affine = S.eq_stride == 1;
-    const float4* __restrict__ rec = S.eq + (size_t)eid * S.eq_stride * 3;
-    float4 A = __ldg(rec), B = __ldg(rec + 1), C = __ldg(rec + 2);
 #pragma unroll (NQ <= 11 ? NQ : 1)
     for (int q = 0; q < NQ; ++q) {
-        if (!affine && q > 0) { A = __ldg(rec + 3 * q); B = __ldg(rec + 3 * q + 1); C = __ldg(rec + 3 * q + 2); }
+        if (!affine && q > 0) { A = ld_hint(rec + 3 * q, stream); B = ld_hint(rec + 3 * q + 1, stream); C = ld_hint(rec + 3 * q + 2, stream); }
         // Jx columns: Jk = sum_i u_i dN_qi[k]
         V3 J0 = mk(0, 0, 0), J1 = mk(0, 0, 0), J2 = mk(0, 0, 0);
 #pragma unroll
@@ -232,6 +252,53 @@ __device__ __forceinline__ void owner_terms(const SceneDev& S, int packed, const
             for (int k = 0; k < 9; ++k) acc[k] += t[k];
         }
     }
+}
+
+// Owner given as a packed (element, local node) id: topology and records from global memory.
+template <int E, int MAT>
+__device__ __forceinline__ void owner_terms(const SceneDev& S, int packed, const float* __restrict__ s_dN, bool mixed,
+                                            float acc[9], float cmp[9]) {
+    constexpr int NE = ElemT<E>::NE;
+    const int eid = packed >> kOwnerShift, r = packed & ((1 << kOwnerShift) - 1);
+    const int* __restrict__ tp = S.topo + (size_t)eid * NE;
+    const unsigned long long keep = policy_keep(), stream = policy_stream();
+    float ux[NE], uy[NE], uz[NE];
+#pragma unroll
+    for (int i = 0; i < NE; ++i) {
+        const float4 t = ld_hint(&S.u[ld_hint(tp + i, stream)], keep);
+        ux[i] = t.x; uy[i] = t.y; uz[i] = t.z;
+    }
+    const float4* __restrict__ rec = S.eq + (size_t)eid * S.eq_stride * 3;
+    const float4 A = ld_hint(rec, stream), B = ld_hint(rec + 1, stream), C = ld_hint(rec + 2, stream);
+    element_terms<E, MAT>(ux, uy, uz, r, A, B, C, rec, S.eq_stride == 1, s_dN, mixed, acc, cmp, stream);
+}
+
+// Owner given as a staged entry (EntryLayout) in shared memory.
+template <int E, int MAT>
+__device__ __forceinline__ void entry_terms(const SceneDev& S, const float* __restrict__ en, const float* __restrict__ s_dN,
+                                            bool mixed, float acc[9], float cmp[9]) {
+    constexpr int NE = ElemT<E>::NE;
+    using L = EntryLayout<NE>;
+    const unsigned long long keep = policy_keep(), stream = policy_stream();
+    float ux[NE], uy[NE], uz[NE];
+#pragma unroll
+    for (int i = 0; i < NE; ++i) {
+        const float4 t = ld_hint(&S.u[__float_as_int(en[L::kIds + i])], keep);
+        ux[i] = t.x; uy[i] = t.y; uz[i] = t.z;
+    }
+    const int r = __float_as_int(en[L::kR]);
+    const bool affine = S.eq_stride == 1;
+    float4 A, B, C;
+    const float4* rec = nullptr;
+    if (affine) {
+        A = make_float4(en[L::kRec], en[L::kRec + 1], en[L::kRec + 2], en[L::kRec + 3]);
+        B = make_float4(en[L::kRec + 4], en[L::kRec + 5], en[L::kRec + 6], en[L::kRec + 7]);
+        C = make_float4(en[L::kRec + 8], en[L::kRec + 9], en[L::kRec + 10], en[L::kRec + 11]);
+    } else {
+        rec = S.eq + (size_t)__float_as_int(en[L::kEid]) * S.eq_stride * 3;
+        A = ld_hint(rec, stream); B = ld_hint(rec + 1, stream); C = ld_hint(rec + 2, stream);
+    }
+    element_terms<E, MAT>(ux, uy, uz, r, A, B, C, rec, affine, s_dN, mixed, acc, cmp, stream);
 }
 
 // Solve of one vertex: damping and inertia terms (compute_correction,
@@ -315,62 +382,112 @@ __device__ __forceinline__ void vertex_epilogue(const SceneDev& S, int vid, cons
     }
 }
 
+// Bounded wait on an mbarrier phase; false when the iteration limit ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned mb, unsigned phase) {
+    unsigned done = 0;
+    for (long it = 0; it < kSpinLimit && !done; ++it)
+        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                     : "=r"(done) : "r"(mb), "r"(phase) : "memory");
+    return done != 0;
+}
+
 // Packed mapping: one lane per (vertex, owner) pair.  The host packs whole vertices of one
-// colour into warp items (at most 32 pairs each), so lanes are busy whatever the valences;
-// each vertex's terms are then summed with a segmented shuffle reduction into its first
-// lane, which runs the epilogue.
+// colour into warp items (at most 32 pairs each, heads = bit mask of each vertex's first
+// pair), so lanes are busy whatever the valences; each vertex's terms are summed with a
+// segmented shuffle reduction into its first lane, which runs the epilogue.  Each warp
+// stages its items' owner entries (node ids, local index, quadrature record; contiguous in
+// slot order) into shared memory with cp.async.bulk, double-buffered on two mbarriers:
+// the next item's entries arrive while the current item computes, leaving the node-
+// displacement gathers as the only dependent global loads.
 template <int E, int MAT>
 __global__ void __launch_bounds__(kBlock) k_vertex_packed(const SceneDev* __restrict__ scenes,
                                                           const VWork* __restrict__ work, int n_work, int mode,
                                                           StepParams P, double* red) {
     constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ;
+    constexpr int EW = EntryLayout<NE>::kWords;
+    constexpr int WPB = kBlock / 32;
     __shared__ __align__(128) float s_dN[((NQ * NE * 3 + 3) / 4) * 4];
     __shared__ __align__(8) unsigned long long s_mbar;
+    __shared__ __align__(8) unsigned long long s_bar[WPB][2];
+    extern __shared__ __align__(128) float s_ent[];   // [WPB][2][32 * EW]
     stage_table(s_dN, gdN<E>(), NQ * NE * 3, &s_mbar, P.error);
     const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const int wpb = kBlock / 32;
-    for (int w = blockIdx.x * wpb + (threadIdx.x >> 5); w < n_work; w += gridDim.x * wpb) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned bar0 = (unsigned)__cvta_generic_to_shared(&s_bar[warp][0]);
+    const unsigned bar1 = (unsigned)__cvta_generic_to_shared(&s_bar[warp][1]);
+    float* buf0 = s_ent + (size_t)warp * 2 * 32 * EW;
+    float* buf1 = buf0 + 32 * EW;
+    if (lane == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    auto issue = [&](int item, int b) {   // lane 0: bulk-copy the item's entries into buffer b
+        const VWork wk = work[item];
+        const float4* src = scenes[wk.scene].ent + (size_t)wk.pair_base * (EW / 4);
+        const unsigned bytes = (unsigned)wk.n_pairs * EW * 4;
+        const unsigned dst = (unsigned)__cvta_generic_to_shared(b ? buf1 : buf0);
+        const unsigned bar = b ? bar1 : bar0;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                     ::"r"(dst), "l"(src), "r"(bytes), "r"(bar) : "memory");
+    };
+    const int stride = gridDim.x * WPB;
+    int w = blockIdx.x * WPB + warp;
+    if (lane == 0 && w < n_work) issue(w, 0);
+    unsigned phase0 = 0, phase1 = 0;
+    for (int k = 0; w < n_work; ++k, w += stride) {
+        const int b = k & 1;
+        if (lane == 0 && w + stride < n_work) issue(w + stride, b ^ 1);
         const VWork wk = work[w];
         const SceneDev& S = scenes[wk.scene];
-        // pair offset of each slot start relative to the item (lane n_slots holds the end)
-        int start = 32;
-        if (lane <= wk.count) start = __ldg(S.own_off + wk.slot_begin + lane) - wk.pair_base;
-        const int n_pairs = __shfl_sync(full, start, wk.count);
-        const unsigned heads = __reduce_or_sync(full, (lane < wk.count) ? (1u << start) : 0u);
-        const unsigned upto = heads & ((2u << lane) - 1u);
-        const int seg = __popc(upto) - 1;
+        float* buf = b ? buf1 : buf0;
+        const bool ok = mbar_wait(b ? bar1 : bar0, b ? phase1 : phase0);
+        if (b) phase1 ^= 1; else phase0 ^= 1;
+        if (!__all_sync(full, ok)) {   // time-out: record it and load this item directly
+            if (lane == 0) atomicOr(P.error, 1);
+            if (lane < wk.n_pairs)
+                for (int j = 0; j < EW; ++j) buf[lane * EW + j] = reinterpret_cast<const float*>(S.ent)[((size_t)wk.pair_base + lane) * EW + j];
+            __syncwarp();
+        }
+        const float* en = buf + lane * EW;
+        const unsigned upto = wk.heads & ((2u << lane) - 1u);
         const int head = 31 - __clz(upto);
-        const unsigned above = heads & ~((2u << lane) - 1u);
-        const int seg_end = above ? __ffs(above) - 1 : n_pairs;
+        const unsigned above = wk.heads & ~((2u << lane) - 1u);
+        const int seg_end = above ? __ffs(above) - 1 : wk.n_pairs;
         int vid = 0;
         bool active = false;
-        if (lane < n_pairs) {
-            vid = __ldg(S.vids + wk.slot_begin + seg);
+        if (lane < wk.n_pairs) {
+            vid = __float_as_int(en[EntryLayout<NE>::kIds + __float_as_int(en[EntryLayout<NE>::kR])]);
             active = mode == 2 || S.mask[vid] != 0;
         }
         float acc[9], cmp[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) { acc[k] = 0.f; cmp[k] = 0.f; }
+        for (int q = 0; q < 9; ++q) { acc[q] = 0.f; cmp[q] = 0.f; }
         const bool mixed = S.precision != 0;
         if (active) {
-            owner_terms<E, MAT>(S, __ldg(S.owners + wk.pair_base + lane), s_dN, mixed, acc, cmp);
+            entry_terms<E, MAT>(S, en, s_dN, mixed, acc, cmp);
             if (mixed) {
 #pragma unroll
-                for (int k = 0; k < 9; ++k) acc[k] -= cmp[k];
+                for (int q = 0; q < 9; ++q) acc[q] -= cmp[q];
             }
         }
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
 #pragma unroll
-            for (int k = 0; k < 9; ++k) {
-                const float o = __shfl_down_sync(full, acc[k], off);
-                if (lane + off < seg_end) acc[k] += o;
+            for (int q = 0; q < 9; ++q) {
+                const float o = __shfl_down_sync(full, acc[q], off);
+                if (lane + off < seg_end) acc[q] += o;
             }
         }
         if (active && lane == head) vertex_epilogue(S, vid, acc, mode, P, red);
+        __syncwarp();   // buffer b is refilled by the next-but-one issue
     }
 }
+
+template <int E> constexpr int packed_smem_bytes() { return (kBlock / 32) * 2 * 32 * EntryLayout<ElemT<E>::NE>::kWords * 4; }
 
 // ------------------------------------------------------------------------ colour kernel
 // mode 0: VBD solve; mode 1: VBD residual (writes |r| reductions); mode 2: explicit force.
@@ -769,7 +886,7 @@ __global__ void k_energy_nodes(const SceneDev* __restrict__ scenes, int scene, d
 
 // ------------------------------------------------------------------------ launchers
 namespace {
-template <class K> int persistent_grid(K kernel, int n_work) {
+template <class K> int persistent_grid(K kernel, int n_work, size_t smem = 0) {
     static int sms = 0;
     if (!sms) {
         int dev = 0;
@@ -777,7 +894,7 @@ template <class K> int persistent_grid(K kernel, int n_work) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kBlock, smem);
     if (per_sm < 1) per_sm = 1;
     const int g = sms * per_sm;
     return n_work < g ? n_work : g;
@@ -795,14 +912,17 @@ void vertex_dispatch(const SceneDev* scenes, const VWork* work, int n_work, int 
                      double* red, cudaStream_t st) {
     if (mode < 0) {   // preparation call: fill the caches only
         if (grid_cap<E, MAT, false>() <= 0) grid_cap<E, MAT, false>() = persistent_grid(k_vertex<E, MAT>, 1 << 30);
-        if (grid_cap<E, MAT, true>() <= 0) grid_cap<E, MAT, true>() = persistent_grid(k_vertex_packed<E, MAT>, 1 << 30);
+        if (grid_cap<E, MAT, true>() <= 0) {
+            cudaFuncSetAttribute(k_vertex_packed<E, MAT>, cudaFuncAttributeMaxDynamicSharedMemorySize, packed_smem_bytes<E>());
+            grid_cap<E, MAT, true>() = persistent_grid(k_vertex_packed<E, MAT>, 1 << 30, packed_smem_bytes<E>());
+        }
         return;
     }
     if (tpv == 0) {
         int cap = grid_cap<E, MAT, true>();
         if (cap <= 0) cap = 148 * 4;
         const int blocks = (n_work + kBlock / 32 - 1) / (kBlock / 32);
-        k_vertex_packed<E, MAT><<<blocks < cap ? blocks : cap, kBlock, 0, st>>>(scenes, work, n_work, mode, P, red);
+        k_vertex_packed<E, MAT><<<blocks < cap ? blocks : cap, kBlock, packed_smem_bytes<E>(), st>>>(scenes, work, n_work, mode, P, red);
         return;
     }
     int cap = grid_cap<E, MAT, false>();

@@ -167,17 +167,19 @@ oct_status ensure_tables(oct_ctx* c, int element) {
 void append_vwork(std::vector<VWork>& out, int scene, int begin, int end, int tpv, const std::vector<int32_t>& own_off) {
     if (tpv > 0) {
         const int vpb = kBlockThreads / tpv;
-        for (int s = begin; s < end; s += vpb) out.push_back({scene, s, std::min(vpb, end - s), 0});
+        for (int s = begin; s < end; s += vpb) out.push_back({scene, s, std::min(vpb, end - s), 0, 0u, 0, 0, 0});
         return;
     }
     int s = begin;
     while (s < end) {
         int pairs = 0, n = 0;
+        unsigned heads = 0;
         while (s + n < end && n < 31 && pairs + (own_off[s + n + 1] - own_off[s + n]) <= 32) {
+            heads |= 1u << pairs;
             pairs += own_off[s + n + 1] - own_off[s + n];
             ++n;
         }
-        out.push_back({scene, s, n, own_off[s]});
+        out.push_back({scene, s, n, own_off[s], heads, pairs, 0, 0});
         s += n;
     }
 }
@@ -429,6 +431,24 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     h.bmaxx = d->box_max[0]; h.bmaxy = d->box_max[1]; h.bmaxz = d->box_max[2];
     h.box_limit = s->box;
     h.precision = s->precision;
+    // owner entries in slot order for the packed mapping (EntryLayout in device.cuh)
+    h.ent = nullptr;
+    if (s->tpv == 0) {
+        const int EW = ((NE + 2 + 12) + 3) / 4 * 4;
+        std::vector<float4> ent((size_t)owners.size() * EW / 4, make_float4(0, 0, 0, 0));
+        for (size_t o = 0; o < owners.size(); ++o) {
+            float* e = reinterpret_cast<float*>(&ent[o * EW / 4]);
+            int32_t* ei = reinterpret_cast<int32_t*>(e);
+            const int eid = owners[o] >> kOwnerShift, r = owners[o] & ((1 << kOwnerShift) - 1);
+            for (int i = 0; i < NE; ++i) ei[i] = topo[(size_t)eid * NE + i];
+            ei[NE] = r;
+            ei[NE + 1] = eid;
+            if (h.eq_stride == 1) std::memcpy(e + NE + 2, &eq[(size_t)eid * 3], 12 * sizeof(float));
+        }
+        float4* entd;
+        if ((st = upload(c, s->mem, entd, ent))) return st;
+        h.ent = entd;
+    }
     if ((st = s->mem.alloc(s->d_scene, 1))) return st;
     OCT_CUDA(c, cudaMemcpy(s->d_scene, &h, sizeof(SceneDev), cudaMemcpyHostToDevice));
     s->pending_host = s->has_v0 ? 1 : 0;
@@ -619,6 +639,7 @@ oct_status oct_scene_footprint(const oct_scene_desc* d, size_t* bytes) {
     const size_t N = d->n_nodes, E = d->n_elements;
     size_t b = N * (6 * sizeof(float4) + 3 * sizeof(int)) + (d->rho > 0.f ? 2 * N * sizeof(float4) : 0);
     b += E * ne * sizeof(int) * 2 + E * nq * 3 * sizeof(float4);   // topology, owners, quadrature records
+    b += E * ne * (size_t)(((ne + 2 + 12) + 3) / 4 * 4) * sizeof(float);   // owner entries
     b += (N / 16 + 64) * sizeof(VWork) + (N / 256 + 8) * 2 * sizeof(NWork) + (size_t)std::max(d->n_fixed, 0) * sizeof(int);
     b += 4096;   // descriptors and reduction scratch
     *bytes = b;
