@@ -219,6 +219,23 @@ oct_status oct_batch_group_info(oct_batch* b, int g, int32_t* element, int32_t* 
  * state advances as in an iteration) and returns their total device time (CUDA events). */
 oct_status oct_batch_time_group(oct_batch* b, int g, int sweeps, float dt, float* ms);
 
+/* Allocation-free FP64 elastic energy (no counterpart in the reference; the reference has
+ * no energy evaluator).  For callers that must not allocate device memory when they call
+ * it: a host application whose device memory belongs to its own pool and which forbids
+ * driver allocations inside its frame loop, or a real-time loop that cannot take the
+ * latency and implicit synchronisation of cudaMalloc/cudaFree.  Computes
+ * sum_e sum_q Psi(F) |det J| w_q in FP64 from device positions and rest positions
+ * (n_nodes*3 floats each) and the device topology, writing one double to d_out, in a fixed
+ * summation order (the same bits on every call).  Intermediate storage is a static
+ * per-device array of one double per element, at most 1 << 20 elements (8 MiB); larger
+ * meshes are rejected with OCT_EINVAL.  Calls that overlap on the GPU race on that array.
+ * The first call on a device sets it up (takes the array's device address, uploads the
+ * Hexa_27 tables) and should come before any stream capture.  stream: a cudaStream_t, or
+ * NULL for the default stream.  Nothing is allocated. */
+oct_status oct_elastic_energy_noalloc(int element, int material, const float* d_positions, const float* d_rest_positions,
+                                      const int32_t* d_topology, int n_elements, float young, float poisson,
+                                      double* d_out, void* stream);
+
 /* Device timing of the last oct_scene_step / oct_batch_step (ms, CUDA events). */
 oct_status oct_last_step_ms(oct_ctx* ctx, float* ms);
 /* Number of kernel launches issued by this context since creation. */

@@ -35,7 +35,7 @@ EXPORTS = [
     "oct_color", "oct_last_step_ms", "oct_launch_count", "oct_ctx_stream", "oct_fp32_peak",
     "oct_batch_group_info", "oct_batch_time_group", "oct_scene_set_precision", "oct_scene_footprint",
     "oct_server_create", "oct_server_submit", "oct_server_tick", "oct_server_poll", "oct_server_get_stats",
-    "oct_server_destroy",
+    "oct_server_destroy", "oct_elastic_energy_noalloc",
 ]
 
 
@@ -129,6 +129,8 @@ def lib():
             "oct_server_poll": ([vp, C.c_int64, ip, fp], C.c_int),
             "oct_server_get_stats": ([vp, C.POINTER(ServerStats)], C.c_int),
             "oct_server_destroy": ([vp], C.c_int),
+            "oct_elastic_energy_noalloc": ([C.c_int, C.c_int, vp, vp, vp, C.c_int, C.c_float, C.c_float, vp, vp],
+                                           C.c_int),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
