@@ -49,6 +49,11 @@ def workload_specs(name, seed):
     if name == "p2":   # config 2: P2 beam 64x16x16 over 4x1x1 m, E=1e6, nu=0.49, rho=1100
         return [dict(element=ob.TETRA10, cells=(64, 16, 16), size=(4.0, 1.0, 1.0), young=1e6, poisson=0.49,
                      density=1100.0, v0_sigma=0.05)], 10, 5, FRAME_DT
+    if name in ("cube_p3", "cube_q2"):   # config 3: 1 m cube 32^3, per-element E, top moved down 20 %
+        e = ob.TETRA20 if name == "cube_p3" else ob.HEXA27
+        E = np.exp(rng.uniform(np.log(1e4), np.log(1e6), 32 ** 3 * (6 if e == ob.TETRA20 else 1)))
+        return [dict(element=e, cells=(32, 32, 32), size=(1.0, 1.0, 1.0), young=1e5, poisson=0.45, density=1000.0,
+                     young_per_element=E.astype(np.float32), cube=True)], 10, 2, FRAME_DT
     if name == "cfg1":  # config 1: 8x2x2 P1 beam, E=1e5, nu=0.45, dt=0.01, 1 x 20
         return [dict(element=ob.TETRA, cells=(8, 2, 2), size=(1.0, 0.25, 0.25), young=1e5, poisson=0.45,
                      density=1000.0)], 20, 1, 0.01
@@ -58,10 +63,23 @@ def workload_specs(name, seed):
 def build_scene(ctx, spec, iterations, precision, seed, tpv=0):
     import octopusengine_b200 as ob
     X, T = ob.beam_mesh(spec["element"], spec["cells"], spec["size"])
-    fixed = ob.fixed_by_plane(X, (0.01, 0.0, 0.0), (-1.0, 0.0, 0.0))
+    group = None
+    if spec.get("cube"):   # bottom face: rigid group 0 (static); top face: group 1 (moved)
+        bottom = np.nonzero(X[:, 2] < 1e-6)[0]
+        top = np.nonzero(X[:, 2] > spec["size"][2] - 1e-6)[0]
+        fixed = np.concatenate([bottom, top]).astype(np.int32)
+        group = np.concatenate([np.zeros(len(bottom)), np.ones(len(top))]).astype(np.int32)
+        order = np.argsort(fixed, kind="stable")
+        fixed, group = fixed[order], group[order]
+    else:
+        fixed = ob.fixed_by_plane(X, (0.01, 0.0, 0.0), (-1.0, 0.0, 0.0))
     kw = dict(density=spec["density"], mass_distribution=ob.MASS_FEMSHAPE, material=ob.STABLE_NEOHOOKE,
               young=spec["young"], poisson=spec["poisson"], fixed_ids=fixed, iterations=iterations,
               gravity=(0.0, 0.0, -9.81), precision=precision, threads_per_vertex=tpv)
+    if group is not None:
+        kw["fixed_group"] = group
+    if spec.get("young_per_element") is not None:
+        kw["young_per_element"] = spec["young_per_element"]
     if spec.get("v0_sigma"):
         kw["initial_velocity"] = np.random.default_rng(seed).normal(0, spec["v0_sigma"], X.shape).astype(np.float32)
     return ob.Scene(ctx, spec["element"], X, T, **kw)
@@ -147,7 +165,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "p2", "cfg1"])
+    ap.add_argument("--workload", default="batched", choices=["batched", "p2", "cfg1", "cube_p3", "cube_q2"])
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -212,8 +230,18 @@ def main():
         if world > 1:
             torch.distributed.barrier()
 
-    for _ in range(args.warmup):
+    cube = bool(specs[0].get("cube"))
+    frame = [0]
+
+    def step_all():
+        if cube:   # top face moved down 20 % of the height over 50 frames, then held
+            frame[0] += 1
+            for s in scenes:
+                s.set_fixation((0.0, 0.0, -0.2 * min(frame[0], 50) / 50.0), group=1)
         batch.step(frame_dt, substeps)
+
+    for _ in range(args.warmup):
+        step_all()
     torch.cuda.synchronize()
 
     # ---- timed region: K batched steps, per-step events on the library's stream
@@ -224,7 +252,7 @@ def main():
     with ClockSampler(device) as clocks:
         ev[0].record(stream)
         for k in range(args.steps):
-            batch.step(frame_dt, substeps)
+            step_all()
             ev[k + 1].record(stream)
         torch.cuda.synchronize()
     barrier()
@@ -248,7 +276,7 @@ def main():
     e_start.record(stream)
     for _ in range(args.steps):
         batch.set_state(host_np)
-        batch.step(frame_dt, substeps)
+        step_all()
         batch.get_state(host_np)
     e_end.record(stream)
     torch.cuda.synchronize()

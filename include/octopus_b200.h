@@ -80,6 +80,8 @@ typedef struct oct_scene_desc {
     float gravity[3];
     int32_t n_fixed;                /* fixed-node list (GPU_Fix_Constraint ids)... */
     const int32_t* fixed_ids;
+    const int32_t* fixed_group;     /* NULL, or per fixed id its rigid group 0..3 (one
+                                       GPU_Fix_Constraint each; the reference scenes attach two) */
     int32_t fix_by_plane;           /* ...or nodes with dot(p - origin, normal) > 0 (Area::Plane) */
     float plane_origin[3], plane_normal[3];
     const float* initial_velocity;  /* NULL or n_nodes*3 */
@@ -125,8 +127,11 @@ oct_status oct_scene_get_coloring(oct_scene* s, int32_t* colors, int32_t* vertex
 /* Lumped masses used by the scene (compute_fem_mass). */
 oct_status oct_scene_get_masses(oct_scene* s, float* out_n);
 /* Move the fixed nodes rigidly: p = offset + com + R (init_p - com), R column-major 3x3
- * (GPU_Fix_Constraint axis, octopus/src/GPU/GPU_Constraint.cu:108-112). */
+ * (GPU_Fix_Constraint axis, octopus/src/GPU/GPU_Constraint.cu:108-112).  _group addresses
+ * one of the four rigid groups (oct_scene_set_fixation is group 0); batches holding the
+ * scene see the change. */
 oct_status oct_scene_set_fixation(oct_scene* s, const float offset[3], const float rotation[9]);
+oct_status oct_scene_set_fixation_group(oct_scene* s, int group, const float offset[3], const float rotation[9]);
 /* Switches the scene between OCT_PREC_PLAIN and OCT_PREC_MIXED for its own steps (a batch
  * keeps the precision its scenes had when the batch was created). */
 oct_status oct_scene_set_precision(oct_scene* s, int precision);

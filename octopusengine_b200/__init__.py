@@ -94,6 +94,10 @@ def make_desc(element, positions, topology, **kw):
             keep.append(a)
             d.fixed_ids = capi.ptr(a, C.c_int32) if len(a) else None
             d.n_fixed = len(a)
+        elif k == "fixed_group":
+            a = np.ascontiguousarray(v, np.int32).ravel()
+            keep.append(a)
+            d.fixed_group = capi.ptr(a, C.c_int32) if len(a) else None
         elif k in ("gravity", "plane_origin", "plane_normal", "box_min", "box_max"):
             setattr(d, k, (C.c_float * 3)(*v))
         else:
@@ -160,12 +164,12 @@ class Scene:
         capi.check(capi.lib().oct_scene_get_masses(self._h, capi.ptr(m, C.c_float)), "oct_scene_get_masses")
         return m
 
-    def set_fixation(self, offset=(0, 0, 0), rotation=None):
+    def set_fixation(self, offset=(0, 0, 0), rotation=None, group=0):
         off = np.asarray(offset, np.float32)
         rot = np.eye(3, dtype=np.float32) if rotation is None else np.asarray(rotation, np.float32)
         rot = np.ascontiguousarray(rot.T)   # column-major
-        capi.check(capi.lib().oct_scene_set_fixation(self._h, capi.ptr(off, C.c_float), capi.ptr(rot, C.c_float)),
-                   "oct_scene_set_fixation")
+        capi.check(capi.lib().oct_scene_set_fixation_group(self._h, group, capi.ptr(off, C.c_float),
+                                                           capi.ptr(rot, C.c_float)), "oct_scene_set_fixation_group")
 
     def set_precision(self, precision):
         capi.check(capi.lib().oct_scene_set_precision(self._h, precision), "oct_scene_set_precision")

@@ -35,7 +35,7 @@ EXPORTS = [
     "oct_color", "oct_last_step_ms", "oct_launch_count", "oct_ctx_stream", "oct_fp32_peak",
     "oct_batch_group_info", "oct_batch_time_group", "oct_scene_set_precision", "oct_scene_footprint",
     "oct_server_create", "oct_server_submit", "oct_server_tick", "oct_server_poll", "oct_server_get_stats",
-    "oct_server_destroy", "oct_elastic_energy_noalloc",
+    "oct_server_destroy", "oct_elastic_energy_noalloc", "oct_scene_set_fixation_group",
 ]
 
 
@@ -59,7 +59,7 @@ class SceneDesc(C.Structure):
         ("density", C.c_float), ("mass_distribution", C.c_int32), ("material", C.c_int32),
         ("young", C.c_float), ("poisson", C.c_float), ("young_per_element", C.POINTER(C.c_float)),
         ("damping", C.c_float), ("gravity", C.c_float * 3), ("n_fixed", C.c_int32),
-        ("fixed_ids", C.POINTER(C.c_int32)), ("fix_by_plane", C.c_int32), ("plane_origin", C.c_float * 3),
+        ("fixed_ids", C.POINTER(C.c_int32)), ("fixed_group", C.POINTER(C.c_int32)), ("fix_by_plane", C.c_int32), ("plane_origin", C.c_float * 3),
         ("plane_normal", C.c_float * 3), ("initial_velocity", C.POINTER(C.c_float)), ("iterations", C.c_int32),
         ("rho", C.c_float), ("vbd_version", C.c_int32), ("target_color", C.c_int32), ("color_algo", C.c_int32),
         ("order_mode", C.c_int32), ("seed", C.c_uint64), ("global_damping", C.c_float), ("precision", C.c_int32),
@@ -103,6 +103,7 @@ def lib():
             "oct_scene_get_coloring": ([vp, ip, ip], C.c_int),
             "oct_scene_get_masses": ([vp, fp], C.c_int),
             "oct_scene_set_fixation": ([vp, fp, fp], C.c_int),
+            "oct_scene_set_fixation_group": ([vp, C.c_int, fp, fp], C.c_int),
             "oct_scene_energy": ([vp, dp], C.c_int),
             "oct_scene_residual": ([vp, C.c_float, dp], C.c_int),
             "oct_batch_create": ([vp, pp, C.c_int, pp], C.c_int),

@@ -28,6 +28,7 @@ namespace octb {
 constexpr int kMaxNE = 27;
 constexpr int kMaxNQ = 27;
 constexpr int kOwnerShift = 5;
+constexpr int kFixGroups = 4;
 
 struct SceneDev {
     float4* u;          // displacement, per node
@@ -45,14 +46,13 @@ struct SceneDev {
     const int* own_off; // n_nodes + 1, slot order
     const int* owners;  // packed (eid << 5) | r
     const int* fixed;   // n_fixed node ids
+    const int* fixed_group;            // n_fixed rigid-group indices
+    const float* fix;                  // kFixGroups x 16: com (3), offset (3), rotation (9, column-major), pad
     int n_nodes, n_elements, n_fixed, element;
     int eq_stride;                     // records per element: NQ, or 1 for affine elements
     const float4* ent;                 // owner entries in slot order (EntryLayout), or null
     float damping;      // k_d
     float gx, gy, gz;
-    float comx, comy, comz;            // fixed-set centre of mass (float, as the reference)
-    float offx, offy, offz;            // fixation offset
-    float rot[9];                      // fixation rotation, column-major
     float bminx, bminy, bminz, bmaxx, bmaxy, bmaxz;
     int box_limit;
     int precision;                     // 0 plain, 1 mixed

@@ -399,8 +399,11 @@ __device__ __forceinline__ bool mbar_wait(unsigned mb, unsigned phase) {
 // slot order) into shared memory with cp.async.bulk, double-buffered on two mbarriers:
 // the next item's entries arrive while the current item computes, leaving the node-
 // displacement gathers as the only dependent global loads.
+// Resident blocks per SM each element type is compiled for (register cap without spills).
+template <int E> struct MinBlocks { static constexpr int value = E == 3 ? 8 : (E == 7 ? 5 : (E == 6 ? 4 : (E == 8 ? 3 : 2))); };
+
 template <int E, int MAT>
-__global__ void __launch_bounds__(kBlock) k_vertex_packed(const SceneDev* __restrict__ scenes,
+__global__ void __launch_bounds__(kBlock, MinBlocks<E>::value) k_vertex_packed(const SceneDev* __restrict__ scenes,
                                                           const VWork* __restrict__ work, int n_work, int mode,
                                                           StepParams P, double* red) {
     constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ;
@@ -620,13 +623,14 @@ __global__ void k_constraints(const SceneDev* __restrict__ scenes, const NWork* 
     const int k = wk.begin + threadIdx.x;
     if (!box_pass) {
         const int id = S.fixed[k];
+        const float* G = S.fix + 16 * S.fixed_group[k];   // com, offset, rotation
         const float4 X = S.X[id];
-        const float dx = X.x - S.comx, dy = X.y - S.comy, dz = X.z - S.comz;
-        const float* R = S.rot;
+        const float dx = X.x - G[0], dy = X.y - G[1], dz = X.z - G[2];
+        const float* R = G + 6;
         const float rx = R[0] * dx + R[3] * dy + R[6] * dz;
         const float ry = R[1] * dx + R[4] * dy + R[7] * dz;
         const float rz = R[2] * dx + R[5] * dy + R[8] * dz;
-        const float tx = (S.offx + S.comx) + rx, ty = (S.offy + S.comy) + ry, tz = (S.offz + S.comz) + rz;
+        const float tx = (G[3] + G[0]) + rx, ty = (G[4] + G[1]) + ry, tz = (G[5] + G[2]) + rz;
         S.u[id] = make_float4(tx - X.x, ty - X.y, tz - X.z, 0.f);
         S.v[id] = make_float4(0.f, 0.f, 0.f, 0.f);
         S.mask[id] = 0;

@@ -95,7 +95,9 @@ struct oct_scene {
     std::vector<int32_t> colors, vids, color_off;   // colour-sorted slots
     std::vector<int32_t> own_off;                    // owner CSR offsets in slot order (host copy)
     std::vector<float> masses, X;
-    std::vector<int32_t> fixed;
+    std::vector<int32_t> fixed, fixed_group;
+    float fix_host[kFixGroups * 16] = {0};
+    float* d_fix = nullptr;
     // device
     SceneDev h{};
     SceneDev* d_scene = nullptr;
@@ -268,9 +270,28 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
         for (int id : s->fixed) if (id < 0 || id >= N) return fail(c, OCT_EINVAL, "fixed id out of range");
     }
     s->n_fixed = (int)s->fixed.size();
-    float cx = 0, cy = 0, cz = 0;
-    for (int id : s->fixed) { cx += d->positions[3 * id]; cy += d->positions[3 * id + 1]; cz += d->positions[3 * id + 2]; }
-    if (s->n_fixed) { cx /= (float)s->n_fixed; cy /= (float)s->n_fixed; cz /= (float)s->n_fixed; }
+    s->fixed_group.assign(s->n_fixed, 0);
+    if (d->fixed_group && !d->fix_by_plane)
+        for (int k = 0; k < s->n_fixed; ++k) {
+            s->fixed_group[k] = d->fixed_group[k];
+            if (d->fixed_group[k] < 0 || d->fixed_group[k] >= kFixGroups) return fail(c, OCT_EINVAL, "fixed group out of range");
+        }
+    // per group: centre of mass in float as GPU_Fix_Constraint (GPU_Constraint.cu:94-107),
+    // zero offset, identity rotation
+    for (int g = 0; g < kFixGroups; ++g) {
+        float cx = 0, cy = 0, cz = 0;
+        int cnt = 0;
+        for (int k = 0; k < s->n_fixed; ++k) {
+            if (s->fixed_group[k] != g) continue;
+            const int id = s->fixed[k];
+            cx += d->positions[3 * id]; cy += d->positions[3 * id + 1]; cz += d->positions[3 * id + 2];
+            ++cnt;
+        }
+        if (cnt) { cx /= (float)cnt; cy /= (float)cnt; cz /= (float)cnt; }
+        float* G = s->fix_host + 16 * g;
+        G[0] = cx; G[1] = cy; G[2] = cz;
+        for (int k = 0; k < 9; ++k) G[6 + k] = (k % 4 == 0) ? 1.f : 0.f;
+    }
 
     // precompute per (element, quadrature point) in FP64 (GPU_FEM::build_fem_const,
     // octopus/src/GPU/GPU_FEM.cu:176-215) with the Lame parameters of GPU_FEM.cu:162-163
@@ -418,15 +439,15 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     if ((st = upload(c, s->mem, maskd, mask)) || (st = upload(c, s->mem, topod, topo)) || (st = upload(c, s->mem, eqd, eq)) ||
         (st = upload(c, s->mem, vidsd, slot_vids)) || (st = upload(c, s->mem, offd, own_off)) || (st = upload(c, s->mem, ownd, owners)))
         return st;
-    if (s->n_fixed && (st = upload(c, s->mem, fixd, s->fixed))) return st;
+    int* fgd = nullptr;
+    if (s->n_fixed && ((st = upload(c, s->mem, fixd, s->fixed)) || (st = upload(c, s->mem, fgd, s->fixed_group)))) return st;
+    if ((st = upload(c, s->mem, s->d_fix, std::vector<float>(s->fix_host, s->fix_host + kFixGroups * 16)))) return st;
     h.u = u; h.u_last = ul; h.y = y; h.v = v; h.u_new = un; h.prev1 = p1; h.prev2 = p2; h.mask = maskd; h.X = Xd;
     h.topo = topod; h.eq = eqd; h.vids = vidsd; h.own_off = offd; h.owners = ownd; h.fixed = fixd;
+    h.fixed_group = fgd; h.fix = s->d_fix;
     h.n_nodes = N; h.n_elements = E; h.n_fixed = s->n_fixed; h.element = d->element;
     h.damping = d->damping;
     h.gx = d->gravity[0]; h.gy = d->gravity[1]; h.gz = d->gravity[2];
-    h.comx = cx; h.comy = cy; h.comz = cz;
-    h.offx = h.offy = h.offz = 0.f;
-    for (int k = 0; k < 9; ++k) h.rot[k] = (k % 4 == 0) ? 1.f : 0.f;
     h.bminx = d->box_min[0]; h.bminy = d->box_min[1]; h.bminz = d->box_min[2];
     h.bmaxx = d->box_max[0]; h.bmaxy = d->box_max[1]; h.bmaxz = d->box_max[2];
     h.box_limit = s->box;
@@ -736,13 +757,18 @@ oct_status oct_scene_get_masses(oct_scene* s, float* out) {
     return OCT_OK;
 }
 
-oct_status oct_scene_set_fixation(oct_scene* s, const float offset[3], const float rotation[9]) {
-    if (!s) return OCT_EINVAL;
-    if (offset) { s->h.offx = offset[0]; s->h.offy = offset[1]; s->h.offz = offset[2]; }
-    if (rotation) std::copy(rotation, rotation + 9, s->h.rot);
-    OCT_CUDA(s->ctx, cudaMemcpyAsync(s->d_scene, &s->h, sizeof(SceneDev), cudaMemcpyHostToDevice, s->ctx->stream));
+oct_status oct_scene_set_fixation_group(oct_scene* s, int group, const float offset[3], const float rotation[9]) {
+    if (!s || group < 0 || group >= kFixGroups) return OCT_EINVAL;
+    float* G = s->fix_host + 16 * group;
+    if (offset) { G[3] = offset[0]; G[4] = offset[1]; G[5] = offset[2]; }
+    if (rotation) std::copy(rotation, rotation + 9, G + 6);
+    OCT_CUDA(s->ctx, cudaMemcpyAsync(s->d_fix + 16 * group, G, 16 * sizeof(float), cudaMemcpyHostToDevice, s->ctx->stream));
     OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
     return OCT_OK;
+}
+
+oct_status oct_scene_set_fixation(oct_scene* s, const float offset[3], const float rotation[9]) {
+    return oct_scene_set_fixation_group(s, 0, offset, rotation);
 }
 
 oct_status oct_scene_set_precision(oct_scene* s, int precision) {

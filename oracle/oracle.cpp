@@ -644,8 +644,9 @@ template <class T> struct State {
     std::vector<T> m, w;
     std::vector<int> mask;
     V3<T> g;
-    std::vector<int> fixed;
-    V3<T> com;
+    std::vector<int> fixed, fgroup;
+    V3<T> com[4], off[4];
+    M3<T> R[4];
     bool box = false;
     V3<T> bmin, bmax;
 };
@@ -670,10 +671,22 @@ template <class T> void init_state(const orc_desc* d, State<T>& s) {
     s.mask.assign(s.n, 1);
     s.g = {(T)d->gravity[0], (T)d->gravity[1], (T)d->gravity[2]};
     s.fixed.assign(d->fixed_ids, d->fixed_ids + d->n_fixed);
-    V3<float> c;
-    for (int id : s.fixed) c = c + V3<float>(d->positions[3 * id], d->positions[3 * id + 1], d->positions[3 * id + 2]);
-    if (!s.fixed.empty()) c = c / float(s.fixed.size());
-    s.com = {(T)c.x, (T)c.y, (T)c.z};
+    s.fgroup.assign(s.fixed.size(), 0);
+    if (d->fixed_group) for (size_t k = 0; k < s.fixed.size(); ++k) s.fgroup[k] = d->fixed_group[k];
+    for (int g = 0; g < 4; ++g) {   // float centre of mass per group (GPU_Constraint.cu:94-107)
+        V3<float> c;
+        int cnt = 0;
+        for (size_t k = 0; k < s.fixed.size(); ++k) {
+            if (s.fgroup[k] != g) continue;
+            const int id = s.fixed[k];
+            c = c + V3<float>(d->positions[3 * id], d->positions[3 * id + 1], d->positions[3 * id + 2]);
+            ++cnt;
+        }
+        if (cnt) c = c / float(cnt);
+        s.com[g] = {(T)c.x, (T)c.y, (T)c.z};
+        s.off[g] = V3<T>();
+        s.R[g] = M3<T>(T(1));
+    }
     s.box = d->box_limit != 0;
     s.bmin = {(T)d->box_min[0], (T)d->box_min[1], (T)d->box_min[2]};
     s.bmax = {(T)d->box_max[0], (T)d->box_max[1], (T)d->box_max[2]};
@@ -682,10 +695,9 @@ template <class T> void init_state(const orc_desc* d, State<T>& s) {
 // kernel_constraint_fix (GPU_Constraint.cu:8-20) with identity rotation and zero offset,
 // then kernel_constraint_box_limit (:80-92) when enabled.
 template <class T> void apply_constraints(State<T>& s) {
-    const M3<T> R(T(1));
-    const V3<T> off;
-    for (int id : s.fixed) {
-        s.p[id] = off + s.com + R * (s.init_p[id] - s.com);
+    for (size_t k = 0; k < s.fixed.size(); ++k) {
+        const int id = s.fixed[k], g = s.fgroup[k];
+        s.p[id] = s.off[g] + s.com[g] + s.R[g] * (s.init_p[id] - s.com[g]);
         s.v[id] = V3<T>();
         s.f[id] = V3<T>();
         s.mask[id] = 0;
@@ -1147,6 +1159,11 @@ template <class T> Explicit<T>* explicit_create_t(const orc_desc* d) {
     return x;
 }
 
+template <class T> void set_fix(State<T>& s, int g, const float* off, const float* rot) {
+    if (off) s.off[g] = {(T)off[0], (T)off[1], (T)off[2]};
+    if (rot) for (int j = 0; j < 3; ++j) s.R[g][j] = {(T)rot[3 * j], (T)rot[3 * j + 1], (T)rot[3 * j + 2]};
+}
+
 }  // namespace orc
 
 using namespace orc;
@@ -1294,6 +1311,21 @@ int orc_vbd_step(void* hv, float frame_dt, int substeps) {
     for (int k = 0; k < substeps; ++k) {
         if (h->kind == 1) vbd_substep(*(VBD<double>*)h->ptr, (double)sub);
         else vbd_substep(*(VBD<float>*)h->ptr, sub);
+    }
+    return 0;
+}
+
+int orc_set_fixation(void* hv, int g, const float* off, const float* rot) {
+    Handle* h = (Handle*)hv;
+    if (!h || g < 0 || g > 3) return -1;
+    switch (h->kind) {
+        case 0: set_fix(((VBD<float>*)h->ptr)->s, g, off, rot); break;
+        case 1: set_fix(((VBD<double>*)h->ptr)->s, g, off, rot); break;
+        case 2: set_fix(((XPBD<float>*)h->ptr)->s, g, off, rot); break;
+        case 3: set_fix(((XPBD<double>*)h->ptr)->s, g, off, rot); break;
+        case 4: set_fix(((Explicit<float>*)h->ptr)->s, g, off, rot); break;
+        case 5: set_fix(((Explicit<double>*)h->ptr)->s, g, off, rot); break;
+        default: return -1;
     }
     return 0;
 }

@@ -36,6 +36,7 @@ typedef struct orc_desc {
     float gravity[3];
     int32_t n_fixed;
     const int32_t* fixed_ids;
+    const int32_t* fixed_group;     /* NULL or per fixed id its rigid group 0..3 */
     const float* initial_velocity;  /* NULL or n_nodes*3 */
     /* VBD */
     int32_t iterations;
@@ -75,6 +76,10 @@ int orc_vbd_set(void* h, int what, const double* in);
 int orc_vbd_energy(void* h, double* parts);         /* kinetic, elastic, gravity, total */
 int orc_vbd_residual(void* h, float dt, double* out_norms); /* [sum |r|, max |r|] of free nodes */
 void orc_vbd_destroy(void* h);
+
+/* Rigid motion of fixation group g (GPU_Fix_Constraint axis): p = offset + com + R (X - com),
+ * R column-major; works on VBD, XPBD and explicit handles. */
+int orc_set_fixation(void* h, int group, const float* offset, const float* rotation);
 
 /* Reference CPU VBD (VertexBlockDescent.cpp + VBD_FEM.cpp): single-thread Gauss-Seidel in
  * vertex order with the per-iteration full force pass (plot_residual). */

@@ -21,7 +21,8 @@ class OrcDesc(C.Structure):
         ("n_elements", C.c_int32), ("topology", C.POINTER(C.c_int32)), ("masses", C.POINTER(C.c_float)),
         ("material", C.c_int32), ("young", C.c_float), ("poisson", C.c_float),
         ("young_per_element", C.POINTER(C.c_float)), ("damping", C.c_float), ("gravity", C.c_float * 3),
-        ("n_fixed", C.c_int32), ("fixed_ids", C.POINTER(C.c_int32)), ("initial_velocity", C.POINTER(C.c_float)),
+        ("n_fixed", C.c_int32), ("fixed_ids", C.POINTER(C.c_int32)), ("fixed_group", C.POINTER(C.c_int32)),
+        ("initial_velocity", C.POINTER(C.c_float)),
         ("iterations", C.c_int32), ("rho", C.c_float), ("in_place", C.c_int32), ("n_colors", C.c_int32),
         ("colors", C.POINTER(C.c_int32)), ("order_mode", C.c_int32), ("seed", C.c_uint64),
         ("box_limit", C.c_int32), ("box_min", C.c_float * 3), ("box_max", C.c_float * 3),
@@ -53,6 +54,7 @@ def lib():
             getattr(L, "orc_%s_get" % k).argtypes = [vp, C.c_int, dp]
             getattr(L, "orc_%s_destroy" % k).argtypes = [vp]
         L.orc_vbd_set.argtypes = [vp, C.c_int, dp]
+        L.orc_set_fixation.argtypes = [vp, C.c_int, fp, fp]
         L.orc_vbd_energy.argtypes = [vp, dp]
         L.orc_vbd_residual.argtypes = [vp, C.c_float, dp]
         L.orc_cpuvbd_create.argtypes = [C.POINTER(OrcDesc)]
@@ -135,12 +137,14 @@ class Scene:
 
     def __init__(self, element, X, T, m, material=STABLE_NEOHOOKE, young=1e5, poisson=0.45, damping=0.0,
                  gravity=(0, 0, -9.81), fixed=(), v0=None, iterations=20, rho=0.0, in_place=False, colors=None,
-                 n_colors=0, order_mode=0, seed=0, young_per_element=None, box=None, global_damping=0.0):
+                 n_colors=0, order_mode=0, seed=0, young_per_element=None, box=None, global_damping=0.0,
+                 fixed_group=None):
         self.arrays = dict(X=np.ascontiguousarray(X, np.float32), T=np.ascontiguousarray(T, np.int32),
                            m=np.ascontiguousarray(m, np.float32), fixed=np.ascontiguousarray(fixed, np.int32),
                            v0=None if v0 is None else np.ascontiguousarray(v0, np.float32),
                            colors=None if colors is None else np.ascontiguousarray(colors, np.int32),
-                           ype=None if young_per_element is None else np.ascontiguousarray(young_per_element, np.float32))
+                           ype=None if young_per_element is None else np.ascontiguousarray(young_per_element, np.float32),
+                           fgroup=None if fixed_group is None else np.ascontiguousarray(fixed_group, np.int32))
         a = self.arrays
         d = OrcDesc()
         d.element = element
@@ -157,6 +161,7 @@ class Scene:
         d.gravity = (C.c_float * 3)(*gravity)
         d.n_fixed = len(a["fixed"])
         d.fixed_ids = _p(a["fixed"], C.c_int32) if len(a["fixed"]) else None
+        d.fixed_group = _p(a["fgroup"], C.c_int32)
         d.initial_velocity = _p(a["v0"], C.c_float)
         d.iterations = iterations
         d.rho = rho
@@ -190,6 +195,12 @@ class Solver:
         out = np.zeros((self.scene.n, 3)) if what != 4 else np.zeros(self.scene.n)
         getattr(lib(), "orc_%s_get" % self.kind)(self.h, what, _p(out, C.c_double))
         return out
+
+    def set_fixation(self, offset=(0, 0, 0), rotation=None, group=0):
+        off = np.asarray(offset, np.float32)
+        rot = np.eye(3, dtype=np.float32) if rotation is None else np.asarray(rotation, np.float32)
+        rot = np.ascontiguousarray(rot.T)
+        lib().orc_set_fixation(self.h, group, _p(off, C.c_float), _p(rot, C.c_float))
 
     def energy(self):
         e = np.zeros(4)
