@@ -244,13 +244,18 @@ __device__ __forceinline__ void element_terms(const float* ux, const float* uy, 
         const V3 g = mk(dot(m0, dnr), dot(m1, dnr), dot(m2, dnr));
         float t[9];
         material_terms<MAT>(F0, F1, F2, g, lam, mu, V, t);
+        // mixed precision: compensated accumulation of the force, whose sum of nearly
+        // cancelling element terms sets the converged solution; the Hessian only scales
+        // the Newton step and is summed directly
         if (mixed) {
 #pragma unroll
-            for (int k = 0; k < 9; ++k) kadd(acc[k], cmp[k], t[k]);
+            for (int k = 0; k < 3; ++k) kadd(acc[k], cmp[k], t[k]);
         } else {
 #pragma unroll
-            for (int k = 0; k < 9; ++k) acc[k] += t[k];
+            for (int k = 0; k < 3; ++k) acc[k] += t[k];
         }
+#pragma unroll
+        for (int k = 3; k < 9; ++k) acc[k] += t[k];
     }
 }
 
@@ -474,7 +479,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<E>::value) k_vertex_packed(c
             entry_terms<E, MAT>(S, en, s_dN, mixed, acc, cmp);
             if (mixed) {
 #pragma unroll
-                for (int q = 0; q < 9; ++q) acc[q] -= cmp[q];
+                for (int q = 0; q < 3; ++q) acc[q] -= cmp[q];
             }
         }
 #pragma unroll
@@ -526,7 +531,7 @@ __global__ void __launch_bounds__(kBlock) k_vertex(const SceneDev* __restrict__ 
             for (int o = ob + glane; o < oe; o += tpv) owner_terms<E, MAT>(S, __ldg(S.owners + o), s_dN, mixed, acc, cmp);
             if (mixed) {
 #pragma unroll
-                for (int k = 0; k < 9; ++k) acc[k] -= cmp[k];
+                for (int k = 0; k < 3; ++k) acc[k] -= cmp[k];
             }
         }
         for (int off = tpv >> 1; off > 0; off >>= 1) {
