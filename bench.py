@@ -169,7 +169,8 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--tpv", type=int, default=0, help="threads per vertex (0 = per-element default)")
+    ap.add_argument("--tpv", type=int, default=0, help="lanes per vertex (0 = measured default, -1 = packed pair-per-lane mapping)")
+    ap.add_argument("--tpv-elem", default="", help="per-element lanes per vertex, e.g. 3:4,7:-1")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -215,8 +216,9 @@ def main():
     # scene set-up (host colouring etc.) in parallel host threads
     t0 = time.time()
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
-        scenes = list(ex.map(lambda a: build_scene(ctx, a[1], iterations, ob.PREC_MIXED, args.seed + a[0], args.tpv),
-                             enumerate(specs)))
+        per_elem = {int(k): int(v) for k, v in (x.split(":") for x in args.tpv_elem.split(",") if x)}
+        scenes = list(ex.map(lambda a: build_scene(ctx, a[1], iterations, ob.PREC_MIXED, args.seed + a[0],
+                                                   per_elem.get(a[1]["element"], args.tpv)), enumerate(specs)))
     setup_s = time.time() - t0
     batch = ob.Batch(ctx, scenes)
     free_nodes = sum(s.n_nodes - s.n_fixed for s in scenes)
@@ -304,6 +306,12 @@ def main():
     dom = max(groups, key=lambda x: x["flops"])
     sweeps = 10
     ms = C.c_float()
+    for gi in groups:   # every group alone: per-sweep time and algorithmic rates
+        capi.check(capi.lib().oct_batch_time_group(batch._h, gi["g"], 2, frame_dt / substeps, C.byref(ms)), "warm")
+        capi.check(capi.lib().oct_batch_time_group(batch._h, gi["g"], 5, frame_dt / substeps, C.byref(ms)), "time")
+        gi["ms_per_sweep"] = ms.value / 5
+        gi["tflops"] = gi["flops"] / (gi["ms_per_sweep"] * 1e-3) / 1e12
+        gi["gvit_per_s"] = gi["vertices"] / (gi["ms_per_sweep"] * 1e-3) / 1e9
     capi.check(capi.lib().oct_batch_time_group(batch._h, dom["g"], 2, frame_dt / substeps, C.byref(ms)), "warm")
     capi.check(capi.lib().oct_batch_time_group(batch._h, dom["g"], sweeps, frame_dt / substeps, C.byref(ms)),
                "oct_batch_time_group")
@@ -377,6 +385,8 @@ def main():
                     "d2h_bytes_per_step": bytes_state},
             "gpu_launches": int(launches),
             "roofline": roofline,
+            "groups": [{k: g[k] for k in ("element", "vertices", "launches", "ms_per_sweep", "tflops", "gvit_per_s")}
+                       for g in groups],
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
             "setup_s": setup_s,

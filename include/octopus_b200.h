@@ -98,7 +98,9 @@ typedef struct oct_scene_desc {
     int32_t precision;              /* OCT_PREC_* */
     int32_t box_limit;              /* 1: clamp free nodes to [box_min, box_max] each iteration */
     float box_min[3], box_max[3];
-    int32_t threads_per_vertex;     /* 0 = autotune / default */
+    int32_t threads_per_vertex;     /* 0 = measured default per element, -1 = one lane per
+                                       (vertex, owner) pair packed into warps, 1..32 = lanes per
+                                       vertex (power of two) */
 } oct_scene_desc;
 
 /* Context: device, stream, HBM budget (bytes; 0 = 90% of free device memory). */

@@ -500,7 +500,7 @@ template <int E> constexpr int packed_smem_bytes() { return (kBlock / 32) * 2 * 
 // ------------------------------------------------------------------------ colour kernel
 // mode 0: VBD solve; mode 1: VBD residual (writes |r| reductions); mode 2: explicit force.
 template <int E, int MAT>
-__global__ void __launch_bounds__(kBlock) k_vertex(const SceneDev* __restrict__ scenes, const VWork* __restrict__ work,
+__global__ void __launch_bounds__(kBlock, E == 3 ? 6 : 1) k_vertex(const SceneDev* __restrict__ scenes, const VWork* __restrict__ work,
                                                    int n_work, int tpv, int mode, StepParams P, double* red) {
     constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ;
     __shared__ __align__(128) float s_dN[((NQ * NE * 3 + 3) / 4) * 4];
@@ -528,7 +528,32 @@ __global__ void __launch_bounds__(kBlock) k_vertex(const SceneDev* __restrict__ 
         const bool mixed = S.precision != 0;
         if (active) {
             const int ob = __ldg(S.own_off + slot), oe = __ldg(S.own_off + slot + 1);
-            for (int o = ob + glane; o < oe; o += tpv) owner_terms<E, MAT>(S, __ldg(S.owners + o), s_dN, mixed, acc, cmp);
+            if (S.ent) {
+                // owner entries (contiguous per vertex): load the next one while this one computes
+                constexpr int EW = EntryLayout<NE>::kWords;
+                const float4* base = S.ent;
+                const unsigned long long stream = policy_stream();
+                int o = ob + glane;
+                float4 nxt[EW / 4];
+                if (o < oe) {
+#pragma unroll
+                    for (int j = 0; j < EW / 4; ++j) nxt[j] = ld_hint(base + (size_t)o * (EW / 4) + j, stream);
+                }
+                while (o < oe) {
+                    float4 cur[EW / 4];
+#pragma unroll
+                    for (int j = 0; j < EW / 4; ++j) cur[j] = nxt[j];
+                    const int on = o + tpv;
+                    if (on < oe) {
+#pragma unroll
+                        for (int j = 0; j < EW / 4; ++j) nxt[j] = ld_hint(base + (size_t)on * (EW / 4) + j, stream);
+                    }
+                    entry_terms<E, MAT>(S, reinterpret_cast<const float*>(cur), s_dN, mixed, acc, cmp);
+                    o = on;
+                }
+            } else {
+                for (int o = ob + glane; o < oe; o += tpv) owner_terms<E, MAT>(S, __ldg(S.owners + o), s_dN, mixed, acc, cmp);
+            }
             if (mixed) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) acc[k] -= cmp[k];

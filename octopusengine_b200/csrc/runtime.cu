@@ -189,6 +189,16 @@ void append_nwork(std::vector<NWork>& out, int scene, int n) {
     for (int s = 0; s < n; s += kNodeChunk) out.push_back({scene, s, std::min(kNodeChunk, n - s), 0});
 }
 
+// lanes per vertex chosen when the description leaves it at 0 (0 = packed pairs)
+int measured_tpv(int element) {
+    switch (element) {
+        case kTetra: return 4;
+        case kHexa: return 4;
+        case kTetra10: return 2;
+        default: return 0;
+    }
+}
+
 int default_tpv(int element) {
     switch (element) {
         case kTetra: return 8;
@@ -246,9 +256,10 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     s->global_damping = d->global_damping;
     s->box = d->box_limit != 0;
     s->has_v0 = d->initial_velocity != nullptr;
-    s->tpv = d->threads_per_vertex;
-    if (s->tpv != 0 && s->tpv != 1 && s->tpv != 2 && s->tpv != 4 && s->tpv != 8 && s->tpv != 16 && s->tpv != 32)
-        return fail(c, OCT_EINVAL, "threads_per_vertex must be 0 (packed) or a power of two <= 32");
+    s->tpv = d->threads_per_vertex < 0 ? 0 : d->threads_per_vertex;
+    if (d->threads_per_vertex < -1 || (s->tpv != 0 && s->tpv != 1 && s->tpv != 2 && s->tpv != 4 && s->tpv != 8 &&
+                                       s->tpv != 16 && s->tpv != 32))
+        return fail(c, OCT_EINVAL, "threads_per_vertex must be -1 (packed), 0 (default) or a power of two <= 32");
     s->X.assign(d->positions, d->positions + 3 * (size_t)N);
 
     // masses (Cuda_FEM_Dynamic::get_fem_masses)
@@ -389,7 +400,17 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
         std::vector<int> fillp(s->color_off.begin(), s->color_off.end() - 1);
         for (int i = 0; i < N; ++i) slot_vids[fillp[s->colors[i]]++] = i;   // ascending id within colour
     }
-    s->vids = slot_vids;
+    s->vids = slot_vids;   // the reference order (GPU_VBD_FEM::create_buffers), reported by the getters
+    // processing order: within each colour, vertices by decreasing owner count (ascending id
+    // among equals), so the lanes of a warp get similar loads; results do not depend on the
+    // order inside a colour
+    if (d->solver != OCT_SOLVER_XPBD) {
+        std::vector<int32_t> val(N, 0);
+        for (int64_t k = 0; k < (int64_t)E * NE; ++k) val[d->topology[k]]++;
+        for (int k = 0; k + 1 < (int)s->color_off.size(); ++k)
+            std::stable_sort(slot_vids.begin() + s->color_off[k], slot_vids.begin() + s->color_off[k + 1],
+                             [&](int a, int b) { return val[a] > val[b]; });
+    }
 
     // owner CSR in slot order (build_owner_data, GPU_VBD_FEM.cu:677-690: element order)
     std::vector<int32_t> cnt(N, 0);
@@ -409,8 +430,11 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
         own_off[sl + 1] = (int32_t)owners.size();
         max_valence = std::max(max_valence, own_off[sl + 1] - own_off[sl]);
     }
-    // default mapping: one lane per (vertex, owner) pair packed into warps; vertices with
-    // more than 32 owners fall back to a fixed lane group per vertex
+    // default mapping (per-colour sweep times measured on the batched workload): P1 tetrahedra
+    // and Q1 hexahedra use 4 lanes per vertex, P2 tetrahedra 2, each lane looping over a share
+    // of the vertex's owners; the other elements one lane per (vertex, owner) pair packed into
+    // warps; vertices with more than 32 owners fall back to a lane group per vertex
+    if (d->threads_per_vertex == 0) s->tpv = measured_tpv(d->element);
     if (s->tpv == 0 && max_valence > 32) s->tpv = max_valence > 64 ? 32 : default_tpv(d->element);
     s->own_off = own_off;
 
@@ -454,7 +478,7 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     h.precision = s->precision;
     // owner entries in slot order for the packed mapping (EntryLayout in device.cuh)
     h.ent = nullptr;
-    if (s->tpv == 0) {
+    {
         const int EW = ((NE + 2 + 12) + 3) / 4 * 4;
         std::vector<float4> ent((size_t)owners.size() * EW / 4, make_float4(0, 0, 0, 0));
         for (size_t o = 0; o < owners.size(); ++o) {

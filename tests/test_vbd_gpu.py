@@ -91,9 +91,10 @@ def test_initial_velocity_and_chebyshev(ctx):
     assert rel_err(s.get_position(), o64.get(0)) < 1e-5
 
 
-@pytest.mark.parametrize("tpv", [0, 1, 2, 4, 16, 32])
-def test_threads_per_vertex_do_not_change_results(ctx, tpv):
-    s, o32, o64, mesh = pair(ctx, O.TETRA, cells=(6, 2, 2), iterations=5, tpv=tpv)
+@pytest.mark.parametrize("element", [O.TETRA, O.TETRA10])
+@pytest.mark.parametrize("tpv", [-1, 0, 1, 2, 4, 16, 32])
+def test_threads_per_vertex_do_not_change_results(ctx, tpv, element):
+    s, o32, o64, mesh = pair(ctx, element, cells=(6, 2, 2), iterations=5, tpv=tpv)
     s.step(0.01, 1)
     o64.step(0.01, 1)
     assert rel_err(s.get_position(), o64.get(0)) < 1e-5
