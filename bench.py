@@ -14,7 +14,16 @@ its own, FP32, one launch per colour, no graph) on the same scenes and GPU, p50/
 latency, the end-to-end number through the C ABI with host buffers, the roofline of the
 dominant kernel, and the reference CPU VBD path timed on the host cores.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload batched|p2|cfg1]
+Single-scene solver workloads of the P2 beam (64x16x16 hex grid x 6 tets = 98,304 P2 elements,
+140,481 nodes, E=1e6, nu=0.49, rho=1100, x = 0 fixed, v0 ~ N(0, 0.05) from the seed):
+  xpbd_p2      one step = one 1/60 s frame of 5 XPBD sub-steps (the GPU XPBD has no inner
+               iterations), frame captured as a CUDA graph; metric element-projections/s
+               (one projection = both constraints of one element)
+  explicit_p2  one step = 100 symplectic-Euler sub-steps of dt = 1e-5 s, captured as a CUDA
+               graph; metric vertex-steps/s
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                    [--workload batched|p2|cfg1|cube_p3|cube_q2|xpbd_p2|explicit_p2]
 """
 import argparse
 import concurrent.futures as cf
@@ -54,13 +63,17 @@ def workload_specs(name, seed):
         E = np.exp(rng.uniform(np.log(1e4), np.log(1e6), 32 ** 3 * (6 if e == ob.TETRA20 else 1)))
         return [dict(element=e, cells=(32, 32, 32), size=(1.0, 1.0, 1.0), young=1e5, poisson=0.45, density=1000.0,
                      young_per_element=E.astype(np.float32), cube=True)], 10, 2, FRAME_DT
+    if name in ("xpbd_p2", "explicit_p2"):
+        return [dict(element=ob.TETRA10, cells=(64, 16, 16), size=(4.0, 1.0, 1.0), young=1e6, poisson=0.49,
+                     density=1100.0, v0_sigma=0.05)], 1, (5 if name == "xpbd_p2" else 100), \
+            (FRAME_DT if name == "xpbd_p2" else 100 * 1e-5)
     if name == "cfg1":  # config 1: 8x2x2 P1 beam, E=1e5, nu=0.45, dt=0.01, 1 x 20
         return [dict(element=ob.TETRA, cells=(8, 2, 2), size=(1.0, 0.25, 0.25), young=1e5, poisson=0.45,
                      density=1000.0)], 20, 1, 0.01
     raise SystemExit("unknown workload " + name)
 
 
-def build_scene(ctx, spec, iterations, precision, seed, tpv=0):
+def build_scene(ctx, spec, iterations, precision, seed, tpv=0, solver=None):
     import octopusengine_b200 as ob
     X, T = ob.beam_mesh(spec["element"], spec["cells"], spec["size"])
     group = None
@@ -76,6 +89,8 @@ def build_scene(ctx, spec, iterations, precision, seed, tpv=0):
     kw = dict(density=spec["density"], mass_distribution=ob.MASS_FEMSHAPE, material=ob.STABLE_NEOHOOKE,
               young=spec["young"], poisson=spec["poisson"], fixed_ids=fixed, iterations=iterations,
               gravity=(0.0, 0.0, -9.81), precision=precision, threads_per_vertex=tpv)
+    if solver is not None:
+        kw["solver"] = solver
     if group is not None:
         kw["fixed_group"] = group
     if spec.get("young_per_element") is not None:
@@ -120,6 +135,9 @@ class ClockSampler:
         out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
         try:
             rows = [r.split(",") for r in open(self.path).read().strip().split("\n") if r.strip()]
+            if not rows:
+                out["note"] = "timed region shorter than the 100 ms sampling period: no sample"
+                return out
             sm = [float(r[1]) for r in rows]
             out["sm_mhz"] = float(np.median(sm))
             out["sm_max_mhz"] = float(rows[0][2])
@@ -159,13 +177,181 @@ def cpu_reference(specs, iterations, substeps, dt, threads, sample_every, sample
     return vit / secs, secs, desc
 
 
+SOLVER_WORKLOADS = {"xpbd_p2": "xpbd", "explicit_p2": "explicit"}
+
+
+def solver_units(name, scene_or_spec, substeps):
+    """Work units per step of a single-solver workload: element projections or vertex steps."""
+    if SOLVER_WORKLOADS[name] == "xpbd":
+        return scene_or_spec["n_elements"] * substeps
+    return scene_or_spec["free_nodes"] * substeps
+
+
+def cpu_solver_reference(name, spec, substeps, frame_dt, seed):
+    """The workload's solver restated on the CPU (oracle/, GPU semantics, one thread), timed on a
+    bounded sample: one XPBD sub-step or five explicit sub-steps of the full scene."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as O
+    X, T = O.beam_mesh(spec["element"], spec["cells"], spec["size"])
+    m = O.masses(spec["element"], X, T, spec["density"], 1)
+    fixed = O.fixed_by_plane(X, (0.01, 0, 0), (-1, 0, 0))
+    v0 = np.random.default_rng(seed).normal(0, spec["v0_sigma"], X.shape).astype(np.float32)
+    sc = O.Scene(spec["element"], X, T, m, young=spec["young"], poisson=spec["poisson"], fixed=fixed,
+                 gravity=(0, 0, -9.81), v0=v0)
+    kind = SOLVER_WORKLOADS[name]
+    solver = O.Solver(kind, sc)
+    n = 1 if kind == "xpbd" else 5
+    sub = frame_dt / substeps
+    t0 = time.perf_counter()
+    solver.step(sub * n, n)
+    secs = time.perf_counter() - t0
+    units = (len(T) if kind == "xpbd" else len(X) - len(fixed)) * n
+    desc = ("%d %s sub-step(s) of the full scene (%d elements, %d nodes), 1 host thread, the GPU %s path "
+            "restated in C++ (oracle/)" % (n, kind, len(T), len(X), kind))
+    return units / secs, secs, desc
+
+
+def bench_solver(args, world, rank, local, threads):
+    """xpbd_p2 / explicit_p2: one scene, frames replayed from a CUDA graph."""
+    import ctypes as C
+
+    import torch
+    specs, iterations, substeps, frame_dt = workload_specs(args.workload, args.seed)
+    spec = specs[0]
+    kind = SOLVER_WORKLOADS[args.workload]
+    unit = "element-projections/s" if kind == "xpbd" else "vertex-steps/s"
+    metric = "element_projections_per_s" if kind == "xpbd" else "vertex_steps_per_s"
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        vals = []
+        for _ in range(args.warmup + args.steps):
+            v, secs, desc = cpu_solver_reference(args.workload, spec, substeps, frame_dt, args.seed)
+            vals.append(v)
+        v = float(np.median(vals[args.warmup:]))
+        print(json.dumps({"impl": "reference", "metric": metric, "value": v, "unit": unit, "n_gpus": args.gpus,
+                          "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                          "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                          "config": {"workload": args.workload, "scenes": 1, "seed": args.seed},
+                          "cpu_baseline": {"value": v, "unit": unit, "cores": 1, "kind": "port", "sample": desc},
+                          "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    import octopusengine_b200 as ob
+    from octopusengine_b200 import capi
+    ctx = ob.Context(local, 0)
+    solver = ob.SOLVER_XPBD if kind == "xpbd" else ob.SOLVER_EXPLICIT
+    scene = build_scene(ctx, spec, iterations, ob.PREC_PLAIN, args.seed, solver=solver)
+    scene.set_capture(True)
+    info = dict(n_elements=scene.n_elements, free_nodes=scene.n_nodes - scene.n_fixed)
+    units = solver_units(args.workload, info, substeps)
+    stream_ptr = C.c_void_p()
+    capi.lib().oct_ctx_stream(ctx.handle, C.byref(stream_ptr))
+    stream = torch.cuda.ExternalStream(stream_ptr.value, device=local)
+    for _ in range(args.warmup):
+        scene.step(frame_dt, substeps, sync=False)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    l0 = ctx.launch_count()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        ev[0].record(stream)
+        for k in range(args.steps):
+            scene.step(frame_dt, substeps, sync=False)
+            ev[k + 1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    launches = ctx.launch_count() - l0
+    step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    if world > 1:
+        t = torch.tensor([total_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = units * args.steps * world / (total_ms * 1e-3)
+    # end to end: positions and velocities in from pinned host memory, positions out, each step
+    n = scene.n_nodes
+    host_p = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+    host_v = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+    host_p[:] = scene.get_position()
+    host_v[:] = scene.get_velocity()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        scene.set_position(host_p)
+        scene.set_velocity(host_v)
+        scene.step(frame_dt, substeps, sync=False)
+        host_p[:] = scene.get_position()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    e2e_value = units * args.steps * world / (e2e_ms * 1e-3)
+    # roofline of the frame: algorithmic flops and bytes per unit.  Element projection:
+    # 2 Q (36 n_e + 160) + 24 n_e flops.  Explicit vertex step (vertex-centric force): for each
+    # of the vertex's (owner, quadrature point) pairs Jx 18 n_e, F 48, dF/dx 15, P ~45, f 21.
+    ne, nq = 10, 4
+    fp32_peak = C.c_double()
+    capi.lib().oct_fp32_peak(ctx.handle, C.byref(fp32_peak))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    if kind == "xpbd":
+        flops_unit = 2 * nq * (36 * ne + 160) + 24 * ne
+        bytes_unit = 4 * ne + 48 + 2 * 16 * ne   # topology, one affine record, node gather + write-back
+    else:
+        flops_unit = (info["n_elements"] * ne / n) * nq * (18 * ne + 129)
+        bytes_unit = 16 * 4 + 4 * 2   # u, v, y, u_new per node + owner entry stream (amortised)
+    sec = total_ms * 1e-3 / (args.steps * world)
+    ach_tf = flops_unit * units / sec / 1e12
+    ach_gb = bytes_unit * units / sec / 1e9
+    roofline = {"bound": "hbm", "achieved": ach_gb, "peak": hbm_peak, "unit": "GB/s", "frac": ach_gb / hbm_peak,
+                "traffic": None, "kernel": "whole frame graph (%s)" % ("k_xpbd colour launches" if kind == "xpbd"
+                                                                      else "k_vertex force + integrate"),
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
+                "binding_roof": "fp32",
+                "fp32": {"achieved_tflops": ach_tf, "peak_tflops": fp32_peak.value, "frac": ach_tf / fp32_peak.value,
+                         "flops_per_unit": flops_unit}}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, secs, desc = cpu_solver_reference(args.workload, spec, substeps, frame_dt, args.seed)
+        cpu = {"value": v, "unit": unit, "cores": 1, "kind": "port", "sample": desc}
+    if rank == 0:
+        print(json.dumps({
+            "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "scenes": 1, "elements": info["n_elements"],
+                       "free_nodes": info["free_nodes"], "substeps": substeps, "frame_dt": frame_dt,
+                       "seed": args.seed, "l2": "scene state below L2 size; no flush (single-scene workload)",
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "p50_step_ms": float(np.percentile(step_ms, 50)), "p99_step_ms": float(np.percentile(step_ms, 99)),
+            "e2e": {"value": e2e_value, "unit": unit, "h2d_bytes_per_step": 2 * n * 12, "d2h_bytes_per_step": n * 12},
+            "gpu_launches": int(launches), "roofline": roofline, "clocks": clocks.summary(), "cpu_baseline": cpu}))
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "p2", "cfg1", "cube_p3", "cube_q2"])
+    ap.add_argument("--workload", default="batched",
+                    choices=["batched", "p2", "cfg1", "cube_p3", "cube_q2", "xpbd_p2", "explicit_p2"])
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -177,8 +363,11 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    specs, iterations, substeps, frame_dt = workload_specs(args.workload, args.seed)
     threads = os.cpu_count() or 1
+    if args.workload in SOLVER_WORKLOADS:
+        bench_solver(args, world, rank, local, threads)
+        return
+    specs, iterations, substeps, frame_dt = workload_specs(args.workload, args.seed)
 
     if args.impl == "reference":
         if rank != 0:

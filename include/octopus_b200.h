@@ -38,8 +38,11 @@ typedef enum oct_status {
 
 /* Element ids are the reference's Element enum values (octopus/include/Mesh/Elements.h:4-15). */
 enum { OCT_TETRA = 3, OCT_HEXA = 6, OCT_TETRA10 = 7, OCT_TETRA20 = 8, OCT_HEXA27 = 9 };
-/* Material enum (octopus/include/Dynamic/FEM/ContinuousMaterial.h:8-10). */
-enum { OCT_HOOKE = 0, OCT_STVK = 1, OCT_NEOHOOKE = 2, OCT_STABLE_NEOHOOKE = 3 };
+/* Material enum (octopus/include/Dynamic/FEM/ContinuousMaterial.h:8-10).  Corotated and
+ * FixedCorotated exist only as XPBD constraint pairs in the reference (the GPU VBD and explicit
+ * paths evaluate no stress for them); other solvers reject them with OCT_ENOTSUP. */
+enum { OCT_HOOKE = 0, OCT_STVK = 1, OCT_NEOHOOKE = 2, OCT_STABLE_NEOHOOKE = 3, OCT_COROTATED = 4,
+       OCT_FIXED_COROTATED = 5 };
 /* Mass_Distribution (octopus/include/Dynamic/FEM/FEM_Shape.h:693-696). */
 enum { OCT_MASS_UNIFORM = 0, OCT_MASS_FEMSHAPE = 1 };
 /* Solvers. */
@@ -48,6 +51,11 @@ enum { OCT_SOLVER_VBD = 0, OCT_SOLVER_XPBD = 1, OCT_SOLVER_EXPLICIT = 2 };
  * Reduction_Symmetry update in place within a colour; Better_Coloration applies
  * ColorReduction to target_color and updates all vertices of a colour from the same state. */
 enum { OCT_VBD_BASE = 0, OCT_VBD_THREADED_QUADRATURE = 1, OCT_VBD_REDUCTION_SYMMETRY = 2, OCT_VBD_BETTER_COLORATION = 3 };
+/* XPBD_FEM_VERSION (octopus/include/GPU/PBD/GPU_PBD_FEM.h:11-13; GPU_PBD_FEM::step,
+ * octopus/src/GPU/PBD/GPU_PBD_FEM.cu:661-689).  Tetra4 always uses the normalised V0 update;
+ * for other elements XPBD selects V0, Quadrature and OptiShared (the reference default) the raw
+ * V1/V2 update, and OptiGroup projects nothing, as in the reference. */
+enum { OCT_XPBD_XPBD = 0, OCT_XPBD_QUADRATURE = 1, OCT_XPBD_OPTISHARED = 2, OCT_XPBD_OPTIGROUP = 3 };
 /* Colouring algorithms (octopus/include/Tools/Graph.h). */
 enum { OCT_COLOR_DSAT = 0, OCT_COLOR_GREEDY = 1 };
 /* Colour order per iteration: ascending (fixed, reproducible), or a std::shuffle with an
@@ -101,6 +109,7 @@ typedef struct oct_scene_desc {
     int32_t threads_per_vertex;     /* 0 = measured default per element, -1 = one lane per
                                        (vertex, owner) pair packed into warps, 1..32 = lanes per
                                        vertex (power of two) */
+    int32_t xpbd_version;           /* OCT_XPBD_* (default OCT_XPBD_OPTISHARED) */
 } oct_scene_desc;
 
 /* Context: device, stream, HBM budget (bytes; 0 = 90% of free device memory). */
@@ -118,6 +127,11 @@ oct_status oct_scene_destroy(oct_scene* s);
  * asynchronous on the context stream (the reference's GPU_Integrator::step calls). */
 oct_status oct_scene_step(oct_scene* s, float frame_dt, int substeps);
 oct_status oct_scene_sync(oct_scene* s);
+/* Frame graphs (new; the reference launches every kernel from the host): with capture on, a
+ * frame's sub-steps are captured once into a CUDA graph and replayed while frame_dt and
+ * substeps stay the same.  Off by default.  Frames with the shuffled colour order, and the
+ * first frame after a pending initial velocity, still run launch by launch. */
+oct_status oct_scene_set_capture(oct_scene* s, int on);
 /* GPU_ParticleSystem::get_position / get_velocity (synchronous D2H into host arrays). */
 oct_status oct_scene_get_positions(oct_scene* s, float* out_n3);
 oct_status oct_scene_get_velocities(oct_scene* s, float* out_n3);

@@ -35,7 +35,7 @@ using Geometry = std::vector<Vector3>;
 using Topology = std::vector<int>;
 }  // namespace Mesh
 enum Element { Line, Triangle, Quad, Tetra, Pyramid, Prism, Hexa, Tetra10, Tetra20, Hexa27 };
-enum Material { Hooke, StVK, NeoHooke, Stable_NeoHooke };
+enum Material { Hooke, StVK, NeoHooke, Stable_NeoHooke, Corotated, FixedCorotated };
 enum Mass_Distribution { Uniform, FemShape };
 enum VBD_Version { Base, Threaded_Quadrature, Reduction_Symmetry, Better_Coloration };
 enum XPBD_FEM_VERSION { XPBD, Quadrature, OptiShared, OptiGroup };
@@ -193,6 +193,7 @@ struct GPU_Integrator : GPU_Dynamic {
         d.fixed_ids = fixed.empty() ? nullptr : fixed.data();
         fill(d);
         if (auto* v = dynamic_cast<GPU_VBD_FEM*>(fem)) { d.vbd_version = v->version; d.target_color = v->target_color; }
+        if (auto* x = dynamic_cast<GPU_PBD_FEM*>(fem)) d.xpbd_version = x->version;
         oct_ctx* ctx = default_context();
         check(oct_scene_create(ctx, &d, &owned), "oct_scene_create", ctx);
         ps->scene = owned;

@@ -19,10 +19,11 @@ import ctypes as C
 import numpy as np
 
 from . import capi
-from .capi import (COLOR_DSAT, COLOR_GREEDY, ELEMENT_NODES, HEXA, HEXA27, HOOKE, MASS_FEMSHAPE, MASS_UNIFORM,
-                   NEOHOOKE, ORDER_ASCENDING, ORDER_SHUFFLED, PREC_MIXED, PREC_PLAIN, SOLVER_EXPLICIT, SOLVER_VBD,
-                   SOLVER_XPBD, STABLE_NEOHOOKE, STVK, TETRA, TETRA10, TETRA20, VBD_BASE, VBD_BETTER_COLORATION,
-                   VBD_REDUCTION_SYMMETRY, OctError, beam_mesh, color, fixed_by_plane, lumped_masses, shape_table)
+from .capi import (COLOR_DSAT, COLOR_GREEDY, COROTATED, ELEMENT_NODES, FIXED_COROTATED, HEXA, HEXA27, HOOKE,
+                   MASS_FEMSHAPE, MASS_UNIFORM, NEOHOOKE, ORDER_ASCENDING, ORDER_SHUFFLED, PREC_MIXED, PREC_PLAIN,
+                   SOLVER_EXPLICIT, SOLVER_VBD, SOLVER_XPBD, STABLE_NEOHOOKE, STVK, TETRA, TETRA10, TETRA20, VBD_BASE,
+                   VBD_BETTER_COLORATION, VBD_REDUCTION_SYMMETRY, XPBD_OPTIGROUP, XPBD_OPTISHARED, XPBD_QUADRATURE,
+                   XPBD_XPBD, OctError, beam_mesh, color, fixed_by_plane, lumped_masses, shape_table)
 
 __all__ = ["Context", "Scene", "Batch", "Server", "make_desc", "OctError", "beam_mesh", "color", "lumped_masses", "shape_table",
            "fixed_by_plane", "library_path"]
@@ -124,6 +125,10 @@ class Scene:
     @property
     def handle(self):
         return self._h
+
+    def set_capture(self, on=True):
+        """Replay each frame's sub-steps from a captured CUDA graph (oct_scene_set_capture)."""
+        capi.check(capi.lib().oct_scene_set_capture(self._h, int(on)), "oct_scene_set_capture", self.ctx.handle)
 
     def step(self, frame_dt, substeps=1, sync=True):
         capi.check(capi.lib().oct_scene_step(self._h, frame_dt, substeps), "oct_scene_step", self.ctx.handle)

@@ -17,7 +17,8 @@ STATUS = {0: "OCT_OK", 1: "OCT_EINVAL", 2: "OCT_ENOMEM_BUDGET", 3: "OCT_ETIMEDOU
 TETRA, HEXA, TETRA10, TETRA20, HEXA27 = 3, 6, 7, 8, 9
 ELEMENT_NODES = {TETRA: 4, HEXA: 8, TETRA10: 10, TETRA20: 20, HEXA27: 27}
 ELEMENT_QUADRATURE = {TETRA: 1, HEXA: 8, TETRA10: 4, TETRA20: 11, HEXA27: 27}
-HOOKE, STVK, NEOHOOKE, STABLE_NEOHOOKE = 0, 1, 2, 3
+HOOKE, STVK, NEOHOOKE, STABLE_NEOHOOKE, COROTATED, FIXED_COROTATED = 0, 1, 2, 3, 4, 5
+XPBD_XPBD, XPBD_QUADRATURE, XPBD_OPTISHARED, XPBD_OPTIGROUP = 0, 1, 2, 3
 MASS_UNIFORM, MASS_FEMSHAPE = 0, 1
 SOLVER_VBD, SOLVER_XPBD, SOLVER_EXPLICIT = 0, 1, 2
 VBD_BASE, VBD_THREADED_QUADRATURE, VBD_REDUCTION_SYMMETRY, VBD_BETTER_COLORATION = 0, 1, 2, 3
@@ -27,7 +28,8 @@ PREC_PLAIN, PREC_MIXED = 0, 1
 
 EXPORTS = [
     "oct_ctx_create", "oct_ctx_destroy", "oct_last_error", "oct_ctx_memory", "oct_desc_init",
-    "oct_scene_create", "oct_scene_destroy", "oct_scene_step", "oct_scene_sync", "oct_scene_get_positions",
+    "oct_scene_create", "oct_scene_destroy", "oct_scene_step", "oct_scene_sync", "oct_scene_set_capture",
+    "oct_scene_get_positions",
     "oct_scene_get_velocities", "oct_scene_set_positions", "oct_scene_set_velocities", "oct_scene_info",
     "oct_scene_get_coloring", "oct_scene_get_masses", "oct_scene_set_fixation", "oct_scene_energy",
     "oct_scene_residual", "oct_batch_create", "oct_batch_step", "oct_batch_destroy", "oct_batch_set_state",
@@ -64,7 +66,7 @@ class SceneDesc(C.Structure):
         ("rho", C.c_float), ("vbd_version", C.c_int32), ("target_color", C.c_int32), ("color_algo", C.c_int32),
         ("order_mode", C.c_int32), ("seed", C.c_uint64), ("global_damping", C.c_float), ("precision", C.c_int32),
         ("box_limit", C.c_int32), ("box_min", C.c_float * 3), ("box_max", C.c_float * 3),
-        ("threads_per_vertex", C.c_int32),
+        ("threads_per_vertex", C.c_int32), ("xpbd_version", C.c_int32),
     ]
 
 
@@ -95,6 +97,7 @@ def lib():
             "oct_scene_destroy": ([vp], C.c_int),
             "oct_scene_step": ([vp, C.c_float, C.c_int], C.c_int),
             "oct_scene_sync": ([vp], C.c_int),
+            "oct_scene_set_capture": ([vp, C.c_int], C.c_int),
             "oct_scene_get_positions": ([vp, fp], C.c_int),
             "oct_scene_get_velocities": ([vp, fp], C.c_int),
             "oct_scene_set_positions": ([vp, fp], C.c_int),

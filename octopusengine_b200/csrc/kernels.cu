@@ -717,13 +717,81 @@ __global__ void k_commit(const SceneDev* __restrict__ scenes, const VWork* __res
 }
 
 // ------------------------------------------------------------------------ XPBD
-// kernel_XPBD_V0 (GPU_PBD_FEM.cu:60-93): one thread per element of the colour, two
-// constraints per element (volumetric m = 0 with stiffness lambda, deviatoric m = 1 with
-// mu), eval_material pairs of GPU_PBD_FEM_Materials.cu:97-117.  In place: elements of one
-// colour share no node.
+// Coloured element projection of GPU_PBD_FEM::step (GPU_PBD_FEM.cu:640-717).  Elements of one
+// colour share no node, so each is projected in place.  Per element two constraints run in
+// sequence (m = 0 volumetric with stiffness lambda, m = 1 deviatoric with mu), from the
+// eval_material pairs (GPU_PBD_FEM_Materials.cu:97-117).  Two update forms:
+//   normalised (kernel_XPBD_V0, :13-93; every Tetra4 and XPBD_FEM_VERSION::XPBD):
+//     C' = sqrt|C|, grad' = grad / 2C', dl = -C' / (sum w |grad'|^2 + 1/(k dt^2)),
+//     fixed (mask 0) nodes are not moved;
+//   raw (kernel_XPBD_V1/V2, :141-263; Quadrature and OptiShared on other elements):
+//     alpha = 4C/(k dt^2), beta = C < 1e-12 ? 0 : -2C / (sum w |grad|^2 + alpha), every node
+//     moves (the fixation resets fixed nodes after the sweep).
+// Mapping: a group of G lanes of one warp per element.  Lane i gathers node i (registers and
+// shared memory); lane q evaluates quadrature point q (F, the material pair, P~ = P JX_inv^T V
+// into shared memory); lane i then forms grad_i = sum_q P~_q dN_qi.  The sums over q (C) and
+// over nodes (sum w |grad|^2) are butterfly shuffles inside the group.  The reference-element
+// table dN is staged into shared memory by one TMA bulk copy per block.
+
+// Rotation R of F = R S by the quaternion iteration of Mueller et al., "A Robust Method to
+// Extract the Rotational Part of Deformations" (MIG 2016), run as mat3x3_polardecomposition
+// (CUMatrix.cu:75-96) runs it: R from the identity, at most 10 iterations, stop when
+// |omega| < 1e-8, omega = sum_i R_i x F_i * (1/|sum_i R_i . F_i| + 1e-9).  Columns in and out.
+__device__ __forceinline__ void polar_rotation(V3 F0, V3 F1, V3 F2, V3& R0, V3& R1, V3& R2) {
+    float qw = 1.f, qx = 0.f, qy = 0.f, qz = 0.f;
+    R0 = mk(1.f, 0.f, 0.f); R1 = mk(0.f, 1.f, 0.f); R2 = mk(0.f, 0.f, 1.f);
+    for (int it = 0; it < 10; ++it) {
+        const float den = 1.f / fabsf(dot(R0, F0) + dot(R1, F1) + dot(R2, F2)) + 1e-9f;
+        const V3 cs = cross(R0, F0) + cross(R1, F1) + cross(R2, F2);
+        const V3 om = cs * den;
+        const float w = sqrtf(dot(om, om));
+        if (w < 1e-8f) break;
+        const V3 a = mk(om.x / w, om.y / w, om.z / w);
+        float sn, c;
+        sincosf(0.5f * w, &sn, &c);
+        const float dx = a.x * sn, dy = a.y * sn, dz = a.z * sn;
+        const float nw = c * qw - dx * qx - dy * qy - dz * qz;
+        const float nx = c * qx + dx * qw + dy * qz - dz * qy;
+        const float ny = c * qy - dx * qz + dy * qw + dz * qx;
+        const float nz = c * qz + dx * qy - dy * qx + dz * qw;
+        const float inv = 1.f / sqrtf(nw * nw + nx * nx + ny * ny + nz * nz);
+        qw = nw * inv; qx = nx * inv; qy = ny * inv; qz = nz * inv;
+        R0 = mk(1.f - 2.f * (qy * qy + qz * qz), 2.f * (qx * qy + qw * qz), 2.f * (qx * qz - qw * qy));
+        R1 = mk(2.f * (qx * qy - qw * qz), 1.f - 2.f * (qx * qx + qz * qz), 2.f * (qy * qz + qw * qx));
+        R2 = mk(2.f * (qx * qz + qw * qy), 2.f * (qy * qz - qw * qx), 1.f - 2.f * (qx * qx + qy * qy));
+    }
+}
+
 template <int MAT>
 __device__ __forceinline__ void xpbd_pair(int m, V3 F0, V3 F1, V3 F2, float lam, float mu, V3& P0, V3& P1, V3& P2, float& C) {
-    if (MAT == 2 || MAT == 3) {
+    if (MAT == 4 || MAT == 5) {
+        // GPU_PBD_FEM_Materials.cu:67-95, with F = R S from the polar iteration
+        V3 R0, R1, R2;
+        polar_rotation(F0, F1, F2, R0, R1, R2);
+        const V3 S0 = mk(dot(R0, F0), dot(R1, F0), dot(R2, F0)), S1 = mk(dot(R0, F1), dot(R1, F1), dot(R2, F1)),
+                 S2 = mk(dot(R0, F2), dot(R1, F2), dot(R2, F2));
+        const V3 RS0 = R0 * S0.x + R1 * S0.y + R2 * S0.z, RS1 = R0 * S1.x + R1 * S1.y + R2 * S1.z,
+                 RS2 = R0 * S2.x + R1 * S2.y + R2 * S2.z;   // R S = columns of R S
+        if (MAT == 4 && m == 0) {   // C = tr((S - I)^2), P = 2 tr(S - I) R
+            const float a = S0.x - 1.f, b = S1.y - 1.f, c = S2.z - 1.f;
+            C = a * a + b * b + c * c + (S0.y * S1.x + S1.z * S2.y + S2.x * S0.z) * 2.f;
+            const float t = 2.f * (a + b + c);
+            P0 = R0 * t; P1 = R1 * t; P2 = R2 * t;
+        } else if (MAT == 4) {      // C = |S|^2, P = R (2 S - I)
+            C = dot(S0, S0) + dot(S1, S1) + dot(S2, S2);
+            P0 = RS0 * 2.f - R0; P1 = RS1 * 2.f - R1; P2 = RS2 * 2.f - R2;
+        } else if (m == 0) {        // C = (det S - 1)^2, P = 2 (det S - 1) R cof(S)
+            const V3 K0 = cross(S1, S2), K1 = cross(S2, S0), K2 = cross(S0, S1);
+            const float d = dot(S0, K0) - 1.f;
+            C = d * d;
+            P0 = (R0 * K0.x + R1 * K0.y + R2 * K0.z) * (2.f * d);
+            P1 = (R0 * K1.x + R1 * K1.y + R2 * K1.z) * (2.f * d);
+            P2 = (R0 * K2.x + R1 * K2.y + R2 * K2.z) * (2.f * d);
+        } else {                    // C = 2 |S|^2, P = 4 R (S - I)
+            C = 2.f * (dot(S0, S0) + dot(S1, S1) + dot(S2, S2));
+            P0 = (RS0 - R0) * 4.f; P1 = (RS1 - R1) * 4.f; P2 = (RS2 - R2) * 4.f;
+        }
+    } else if (MAT == 2 || MAT == 3) {
         const V3 C0 = cross(F1, F2), C1 = cross(F2, F0), C2 = cross(F0, F1);
         const float J = dot(F0, C0);
         if (m == 0) {
@@ -768,77 +836,137 @@ __device__ __forceinline__ void xpbd_pair(int m, V3 F0, V3 F1, V3 F2, float lam,
     }
 }
 
-template <int E, int MAT>
+// lanes per element: at least one per quadrature point
+template <int E> struct XpbdLanes { static constexpr int G = E == 3 ? 4 : (E == 6 || E == 7 ? 8 : (E == 8 ? 16 : 32)); };
+
+template <int G> __device__ __forceinline__ float group_sum(float v) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <int E, int MAT, bool RAW>
 __global__ void __launch_bounds__(kBlock) k_xpbd(const SceneDev* __restrict__ scenes, const int* __restrict__ elems,
                                                  int begin, int count, int scene, StepParams P) {
-    constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count) return;
+    constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ, G = XpbdLanes<E>::G, GPB = kBlock / G;
+    constexpr int NI = (NE + G - 1) / G;   // nodes per lane
+    static_assert(NQ <= G, "one quadrature point per lane");
+    __shared__ __align__(16) float s_dN[((NQ * NE * 3 + 3) / 4) * 4];
+    __shared__ __align__(16) float4 s_pos[GPB][NE];
+    __shared__ __align__(16) float4 s_P[GPB][NQ][3];
+    __shared__ unsigned long long s_mbar;
+    stage_table(s_dN, gdN<E>(), NQ * NE * 3, &s_mbar, P.error);
+
+    const int lane = threadIdx.x % G, grp = threadIdx.x / G;
+    const int t = blockIdx.x * GPB + grp;
+    const bool active = t < count;   // no early exit: every lane takes part in the shuffles
     const SceneDev& S = scenes[scene];
-    const int eid = elems[begin + t];
+    const int eid = active ? elems[begin + t] : 0;
     const int* tp = S.topo + (size_t)eid * NE;
+    int vid[NI];
+    float4 u[NI];
+    float w[NI];
+    bool mv[NI];
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+        const int i = lane + k * G;
+        vid[k] = -1; u[k] = make_float4(0.f, 0.f, 0.f, 0.f); w[k] = 0.f; mv[k] = false;
+        if (active && i < NE) {
+            vid[k] = tp[i];
+            u[k] = S.u[vid[k]];
+            w[k] = 1.f / S.y[vid[k]].w;
+            mv[k] = RAW || S.mask[vid[k]] != 0;
+        }
+    }
+    // quadrature record of lane q: JX_inv (columns m0 m1 m2), V, lambda, mu
+    const int q = lane;
+    const bool hasq = active && q < NQ;
     const float4* rec = S.eq + (size_t)eid * S.eq_stride * 3;
     const int qs = S.eq_stride == 1 ? 0 : 1;
-    const float* cd = cdN<E>();
+    V3 m0 = mk(0, 0, 0), m1 = m0, m2 = m0;
+    float V = 0.f;
+    if (hasq) {
+        const float4 A = rec[3 * q * qs], B = rec[3 * q * qs + 1], Cr = rec[3 * q * qs + 2];
+        m0 = mk(A.x, A.y, A.z); m1 = mk(A.w, B.x, B.y); m2 = mk(B.z, B.w, Cr.x);
+        V = Cr.y * wq<E>(q);
+    }
+    const float4 L = active ? rec[2] : make_float4(0.f, 0.f, 1.f, 1.f);
+    const float lam = L.z, mu = L.w;
     const float dt2 = P.dt * P.dt;
+
     for (int m = 0; m < 2; ++m) {
-        float ux[NE], uy[NE], uz[NE], gx[NE], gy[NE], gz[NE];
 #pragma unroll
-        for (int i = 0; i < NE; ++i) {
-            const float4 u = S.u[tp[i]];
-            ux[i] = u.x; uy[i] = u.y; uz[i] = u.z; gx[i] = gy[i] = gz[i] = 0.f;
-        }
-        float C = 0.f, lam = 0.f, mu = 0.f;
-        for (int q = 0; q < NQ; ++q) {
-            const float4 A = rec[3 * q * qs], B = rec[3 * q * qs + 1], Cr = rec[3 * q * qs + 2];
-            V3 J0 = mk(0, 0, 0), J1 = mk(0, 0, 0), J2 = mk(0, 0, 0);
+        for (int k = 0; k < NI; ++k)
+            if (lane + k * G < NE) s_pos[grp][lane + k * G] = u[k];
+        __syncwarp();
+        float Cq = 0.f;
+        if (hasq) {
+            V3 J0 = mk(0, 0, 0), J1 = J0, J2 = J0;
 #pragma unroll
             for (int i = 0; i < NE; ++i) {
-                const float d0 = cd[(q * NE + i) * 3], d1 = cd[(q * NE + i) * 3 + 1], d2 = cd[(q * NE + i) * 3 + 2];
-                J0 = J0 + mk(ux[i], uy[i], uz[i]) * d0; J1 = J1 + mk(ux[i], uy[i], uz[i]) * d1; J2 = J2 + mk(ux[i], uy[i], uz[i]) * d2;
+                const float4 p = s_pos[grp][i];
+                const float* d = &s_dN[(q * NE + i) * 3];
+                const V3 pu = mk(p.x, p.y, p.z);
+                J0 = J0 + pu * d[0]; J1 = J1 + pu * d[1]; J2 = J2 + pu * d[2];
             }
-            const V3 m0 = mk(A.x, A.y, A.z), m1 = mk(A.w, B.x, B.y), m2 = mk(B.z, B.w, Cr.x);
-            const float V = Cr.y * wq<E>(q);
-            lam = Cr.z; mu = Cr.w;
-            V3 F0 = J0 * m0.x + J1 * m0.y + J2 * m0.z, F1 = J0 * m1.x + J1 * m1.y + J2 * m1.z, F2 = J0 * m2.x + J1 * m2.y + J2 * m2.z;
+            V3 F0 = J0 * m0.x + J1 * m0.y + J2 * m0.z, F1 = J0 * m1.x + J1 * m1.y + J2 * m1.z,
+               F2 = J0 * m2.x + J1 * m2.y + J2 * m2.z;
             F0.x += 1.f; F1.y += 1.f; F2.z += 1.f;
             V3 P0, P1, P2;
             float en;
             xpbd_pair<MAT>(m, F0, F1, F2, lam, mu, P0, P1, P2, en);
-            C += en * V;
-            // grad_i += P JX_inv^T dN_qi V  =  P (g_qi) V with g_qi = JX_inv^T dN_qi
+            Cq = en * V;
+            // P~ = P JX_inv^T V: column j = sum_k P_k (m_k)_j
+            const V3 T0 = (P0 * m0.x + P1 * m1.x + P2 * m2.x) * V, T1 = (P0 * m0.y + P1 * m1.y + P2 * m2.y) * V,
+                     T2 = (P0 * m0.z + P1 * m1.z + P2 * m2.z) * V;
+            s_P[grp][q][0] = make_float4(T0.x, T0.y, T0.z, 0.f);
+            s_P[grp][q][1] = make_float4(T1.x, T1.y, T1.z, 0.f);
+            s_P[grp][q][2] = make_float4(T2.x, T2.y, T2.z, 0.f);
+        }
+        float C = group_sum<G>(Cq);
+        __syncwarp();
+        V3 g[NI];
+        float ss = 0.f;
 #pragma unroll
-            for (int i = 0; i < NE; ++i) {
-                const V3 dn = mk(cd[(q * NE + i) * 3], cd[(q * NE + i) * 3 + 1], cd[(q * NE + i) * 3 + 2]);
-                const V3 g = mk(dot(m0, dn), dot(m1, dn), dot(m2, dn)) * V;
-                gx[i] += P0.x * g.x + P1.x * g.y + P2.x * g.z;
-                gy[i] += P0.y * g.x + P1.y * g.y + P2.y * g.z;
-                gz[i] += P0.z * g.x + P1.z * g.y + P2.z * g.z;
+        for (int k = 0; k < NI; ++k) {
+            const int i = lane + k * G;
+            g[k] = mk(0, 0, 0);
+            if (i < NE) {
+#pragma unroll
+                for (int qq = 0; qq < NQ; ++qq) {
+                    const float* d = &s_dN[(qq * NE + i) * 3];
+                    const float4 a = s_P[grp][qq][0], b = s_P[grp][qq][1], c = s_P[grp][qq][2];
+                    g[k] = g[k] + mk(a.x, a.y, a.z) * d[0] + mk(b.x, b.y, b.z) * d[1] + mk(c.x, c.y, c.z) * d[2];
+                }
             }
         }
-        // xpbd_convert_to_constraint + xpbd_solve (GPU_PBD_FEM.cu:13-58)
-        C = C < 0.f ? -C : C;
-        C = sqrtf(C);
-        const float ci = C < 1e-12f ? 0.f : 1.f / (2.f * C);
-        float sum = 0.f;
+        const float k_st = m == 0 ? lam : mu;
+        float step;
+        if (RAW) {
 #pragma unroll
-        for (int i = 0; i < NE; ++i) {
-            gx[i] *= ci; gy[i] *= ci; gz[i] *= ci;
-            sum += (gx[i] * gx[i] + gy[i] * gy[i] + gz[i] * gz[i]) / S.y[tp[i]].w;
-        }
-        const float k = m == 0 ? lam : mu;
-        const float alpha = 1.f / (k * dt2);
-        const float dl = -C / (sum + alpha);
+            for (int k = 0; k < NI; ++k) ss += dot(g[k], g[k]) * w[k];
+            const float S2 = group_sum<G>(ss);
+            const float alpha = 4.f * C / (k_st * dt2);
+            step = C < 1e-12f ? 0.f : -2.f * C / (S2 + alpha);
+        } else {
+            C = sqrtf(C < 0.f ? -C : C);
+            const float ci = C < 1e-12f ? 0.f : 1.f / (2.f * C);
 #pragma unroll
-        for (int i = 0; i < NE; ++i) {
-            const int vid = tp[i];
-            if (S.mask[vid] == 0) continue;
-            const float w = dl / S.y[vid].w;
-            float4 u = S.u[vid];
-            u.x += w * gx[i]; u.y += w * gy[i]; u.z += w * gz[i];
-            S.u[vid] = u;
+            for (int k = 0; k < NI; ++k) { g[k] = g[k] * ci; ss += dot(g[k], g[k]) * w[k]; }
+            const float S2 = group_sum<G>(ss);
+            step = -C / (S2 + 1.f / (k_st * dt2));
         }
+#pragma unroll
+        for (int k = 0; k < NI; ++k)
+            if (mv[k]) {
+                const float f = step * w[k];
+                u[k].x += f * g[k].x; u[k].y += f * g[k].y; u[k].z += f * g[k].z;
+            }
+        __syncwarp();   // every lane has read s_pos / s_P before the next constraint rewrites them
     }
+#pragma unroll
+    for (int k = 0; k < NI; ++k)
+        if (vid[k] >= 0 && mv[k]) S.u[vid[k]] = u[k];
 }
 
 // ------------------------------------------------------------------------ FP64 energy
@@ -976,16 +1104,25 @@ void vertex_mat(int mat, const SceneDev* scenes, const VWork* work, int n_work, 
     }
 }
 
-template <int E>
+template <int E, bool RAW>
 void xpbd_mat(int mat, const SceneDev* scenes, const int* elems, int begin, int count, int scene, const StepParams& P,
               cudaStream_t st) {
-    const int grid = (count + kBlock - 1) / kBlock;
+    constexpr int GPB = kBlock / XpbdLanes<E>::G;
+    const int grid = (count + GPB - 1) / GPB;
     switch (mat) {
-        case 0: k_xpbd<E, 0><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
-        case 1: k_xpbd<E, 1><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
-        case 2: k_xpbd<E, 2><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
-        default: k_xpbd<E, 3><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
+        case 0: k_xpbd<E, 0, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
+        case 1: k_xpbd<E, 1, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
+        case 2: k_xpbd<E, 2, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
+        case 3: k_xpbd<E, 3, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
+        case 4: k_xpbd<E, 4, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
+        default: k_xpbd<E, 5, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
     }
+}
+template <int E>
+void xpbd_form(int mat, bool raw, const SceneDev* scenes, const int* elems, int begin, int count, int scene,
+               const StepParams& P, cudaStream_t st) {
+    if (raw) xpbd_mat<E, true>(mat, scenes, elems, begin, count, scene, P, st);
+    else xpbd_mat<E, false>(mat, scenes, elems, begin, count, scene, P, st);
 }
 }  // namespace
 
@@ -1089,15 +1226,15 @@ void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, i
     k_constraints<<<n_work, kNodeChunk, 0, st>>>(scenes, work, n_work, box_pass);
 }
 
-void launch_xpbd(int element, int material, const SceneDev* scenes, const int* elems, int begin, int count, int scene,
-                 const StepParams& P, cudaStream_t st) {
+void launch_xpbd(int element, int material, bool raw, const SceneDev* scenes, const int* elems, int begin, int count,
+                 int scene, const StepParams& P, cudaStream_t st) {
     if (count <= 0) return;
     switch (element) {
-        case 3: xpbd_mat<3>(material, scenes, elems, begin, count, scene, P, st); break;
-        case 6: xpbd_mat<6>(material, scenes, elems, begin, count, scene, P, st); break;
-        case 7: xpbd_mat<7>(material, scenes, elems, begin, count, scene, P, st); break;
-        case 8: xpbd_mat<8>(material, scenes, elems, begin, count, scene, P, st); break;
-        case 9: xpbd_mat<9>(material, scenes, elems, begin, count, scene, P, st); break;
+        case 3: xpbd_form<3>(material, false, scenes, elems, begin, count, scene, P, st); break;   // always V0
+        case 6: xpbd_form<6>(material, raw, scenes, elems, begin, count, scene, P, st); break;
+        case 7: xpbd_form<7>(material, raw, scenes, elems, begin, count, scene, P, st); break;
+        case 8: xpbd_form<8>(material, raw, scenes, elems, begin, count, scene, P, st); break;
+        case 9: xpbd_form<9>(material, raw, scenes, elems, begin, count, scene, P, st); break;
     }
 }
 

@@ -91,6 +91,14 @@ struct oct_scene {
     int iterations = 1, order_mode = 0, tpv = 8, precision = 0;
     float rho = 0.f, global_damping = 0.f;
     bool in_place = true, box = false, has_v0 = false;
+    bool xpbd_raw = true, xpbd_project = true;   // XPBD update form; false: no projection (OptiGroup)
+    // frame graph (oct_scene_set_capture): the sub-steps of one frame, replayed while the
+    // frame's (dt, substeps) stay the same
+    bool capture = false;
+    cudaGraphExec_t frame_exec = nullptr;
+    float frame_dt = -1.f;
+    int frame_substeps = 0;
+    uint64_t frame_launches = 0;
     std::mt19937 rng;
     std::vector<int32_t> colors, vids, color_off;   // colour-sorted slots
     std::vector<int32_t> own_off;                    // owner CSR offsets in slot order (host copy)
@@ -233,9 +241,14 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     s->ne = element_nodes(d->element);
     s->nq = element_quadrature(d->element);
     if (s->ne < 0) return fail(c, OCT_EINVAL, "unsupported element type");
-    if (d->material < 0 || d->material > 3) return fail(c, OCT_EINVAL, "unsupported material");
-    if (d->n_nodes <= 0 || d->n_elements <= 0 || !d->positions || !d->topology) return fail(c, OCT_EINVAL, "empty mesh");
     if (d->solver < 0 || d->solver > 2) return fail(c, OCT_EINVAL, "unknown solver");
+    if (d->material < 0 || d->material > 5) return fail(c, OCT_EINVAL, "unsupported material");
+    if (d->material > 3 && d->solver != OCT_SOLVER_XPBD)
+        return fail(c, OCT_ENOTSUP, "Corotated and FixedCorotated are XPBD-only materials");
+    if (d->xpbd_version < 0 || d->xpbd_version > 3) return fail(c, OCT_EINVAL, "unknown XPBD version");
+    s->xpbd_raw = d->element != kTetra && (d->xpbd_version == OCT_XPBD_QUADRATURE || d->xpbd_version == OCT_XPBD_OPTISHARED);
+    s->xpbd_project = d->element == kTetra || d->xpbd_version != OCT_XPBD_OPTIGROUP;
+    if (d->n_nodes <= 0 || d->n_elements <= 0 || !d->positions || !d->topology) return fail(c, OCT_EINVAL, "empty mesh");
     s->n_nodes = d->n_nodes;
     s->n_elements = d->n_elements;
     const int N = s->n_nodes, E = s->n_elements, NE = s->ne, NQ = s->nq;
@@ -244,7 +257,7 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     if ((int64_t)E >= (1ll << (31 - kOwnerShift))) return fail(c, OCT_EINVAL, "too many elements for one scene");
     oct_status st = ensure_tables(c, d->element);
     if (st) return st;
-    {
+    if (d->solver != OCT_SOLVER_XPBD) {
         std::lock_guard<std::mutex> lock(c->mu);
         prepare_vertex(d->element, d->material);
     }
@@ -575,8 +588,9 @@ void xpbd_substep(oct_scene* s, float dt) {
     StepParams P = base_params(c, dt);
     launch_predict(s->d_scene, s->d_nwork, s->n_nwork, 1, 0, 0, P, st);
     c->launches++;
-    for (int k = 0; k < s->n_colors; ++k) {
-        launch_xpbd(s->element, s->material, s->d_scene, s->d_elems, s->elem_off[k], s->elem_off[k + 1] - s->elem_off[k], 0, P, st);
+    for (int k = 0; k < s->n_colors && s->xpbd_project; ++k) {
+        launch_xpbd(s->element, s->material, s->xpbd_raw, s->d_scene, s->d_elems, s->elem_off[k],
+                    s->elem_off[k + 1] - s->elem_off[k], 0, P, st);
         c->launches++;
     }
     if (s->n_fixed) { launch_constraints(s->d_scene, s->d_fwork, s->n_fwork, 0, st); c->launches++; }
@@ -612,6 +626,19 @@ oct_status read_nodes(oct_scene* s, const float4* d, float* out, bool add_rest) 
     return OCT_OK;
 }
 
+void run_frame(oct_scene* s, float sub, int substeps) {
+    for (int k = 0; k < substeps; ++k) {
+        if (s->solver == OCT_SOLVER_VBD) vbd_substep(s, sub);
+        else if (s->solver == OCT_SOLVER_XPBD) xpbd_substep(s, sub);
+        else explicit_substep(s, sub);
+    }
+}
+void drop_frame_graph(oct_scene* s) {
+    if (s->frame_exec) cudaGraphExecDestroy(s->frame_exec);
+    s->frame_exec = nullptr;
+    s->frame_dt = -1.f;
+    s->frame_substeps = 0;
+}
 }  // namespace
 
 // ============================================================================ C ABI
@@ -632,6 +659,7 @@ void oct_desc_init(oct_scene_desc* d) {
     d->target_color = -1;
     d->color_algo = OCT_COLOR_DSAT;
     d->precision = OCT_PREC_PLAIN;
+    d->xpbd_version = OCT_XPBD_OPTISHARED;
     for (int k = 0; k < 3; ++k) { d->box_min[k] = -1e30f; d->box_max[k] = 1e30f; }
 }
 
@@ -705,6 +733,7 @@ oct_status oct_scene_create(oct_ctx* c, const oct_scene_desc* d, oct_scene** out
 oct_status oct_scene_destroy(oct_scene* s) {
     if (!s) return OCT_EINVAL;
     cudaStreamSynchronize(s->ctx->stream);
+    drop_frame_graph(s);
     s->mem.release();
     delete s;
     return OCT_OK;
@@ -714,14 +743,45 @@ oct_status oct_scene_step(oct_scene* s, float frame_dt, int substeps) {
     if (!s || substeps <= 0 || !(frame_dt > 0.f)) return OCT_EINVAL;
     oct_ctx* c = s->ctx;
     const float sub = frame_dt / (float)substeps;
+    // the first frame after set-up (pending initial velocity) and shuffled colour orders run
+    // launch by launch; otherwise a captured frame is replayed
+    const bool graph = s->capture && s->order_mode != OCT_ORDER_SHUFFLED && !s->pending_host;
+    if (graph && (!s->frame_exec || s->frame_dt != frame_dt || s->frame_substeps != substeps)) {
+        drop_frame_graph(s);
+        const uint64_t l0 = c->launches;
+        OCT_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        run_frame(s, sub, substeps);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        s->frame_launches = c->launches - l0;
+        c->launches = l0;
+        if (e != cudaSuccess) return fail(c, OCT_ECUDA, std::string("frame capture: ") + cudaGetErrorString(e));
+        const cudaError_t ei = cudaGraphInstantiate(&s->frame_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            s->frame_exec = nullptr;
+            return fail(c, OCT_ECUDA, std::string("frame graph: ") + cudaGetErrorString(ei));
+        }
+        s->frame_dt = frame_dt;
+        s->frame_substeps = substeps;
+    }
     cudaEventRecord(c->ev0, c->stream);
-    for (int k = 0; k < substeps; ++k) {
-        if (s->solver == OCT_SOLVER_VBD) vbd_substep(s, sub);
-        else if (s->solver == OCT_SOLVER_XPBD) xpbd_substep(s, sub);
-        else explicit_substep(s, sub);
+    if (graph) {
+        OCT_CUDA(c, cudaGraphLaunch(s->frame_exec, c->stream));
+        c->launches += s->frame_launches;
+    } else {
+        run_frame(s, sub, substeps);
     }
     cudaEventRecord(c->ev1, c->stream);
     OCT_CUDA(c, cudaGetLastError());
+    return OCT_OK;
+}
+
+oct_status oct_scene_set_capture(oct_scene* s, int on) {
+    if (!s) return OCT_EINVAL;
+    OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    s->capture = on != 0;
+    drop_frame_graph(s);
     return OCT_OK;
 }
 
@@ -806,6 +866,7 @@ oct_status oct_scene_set_precision(oct_scene* s, int precision) {
 
 oct_status oct_scene_energy(oct_scene* s, double out[4]) {
     if (!s || !out) return OCT_EINVAL;
+    if (s->material > OCT_STABLE_NEOHOOKE) return fail(s->ctx, OCT_ENOTSUP, "no energy density for this material");
     oct_ctx* c = s->ctx;
     OCT_CUDA(c, cudaMemsetAsync(s->d_red, 0, 4 * sizeof(double), c->stream));
     launch_energy(s->element, s->material, s->d_scene, 0, s->n_nodes, s->n_elements, s->d_red, c->d_error, c->stream);

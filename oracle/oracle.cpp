@@ -510,7 +510,7 @@ static void color_reduction(const Graph& g, std::vector<int>& colors, int target
 }
 
 // ----------------------------------------------------------------------------- materials
-enum Material { Hooke = 0, StVK = 1, NeoHooke = 2, StableNeoHooke = 3 };
+enum Material { Hooke = 0, StVK = 1, NeoHooke = 2, StableNeoHooke = 3, Corotated = 4, FixedCorotated = 5 };
 
 // PK1 stresses, GPU_FEM_Material.cu:5-36
 template <class T> M3<T> pk1(int mat, T lambda, T mu, const M3<T>& F) {
@@ -600,7 +600,7 @@ template <class T> struct Fem {
 // V = |det J| w_q, JX_inv = J^-1.  Lame parameters from (E, nu) (GPU_FEM.cu:162-163).
 template <class T> bool build_fem(const orc_desc* d, Fem<T>& f) {
     Shape s;
-    if (!build_shape(d->element, s)) return false;
+    if (!build_shape(d->element, s) || d->material < Hooke || d->material > FixedCorotated) return false;
     f.elem = d->element; f.ne = s.nb; f.nq = s.nq; f.n_elem = d->n_elements; f.material = d->material;
     f.topo.assign(d->topology, d->topology + (size_t)f.ne * f.n_elem);
     for (int q = 0; q < f.nq; ++q) {
@@ -986,9 +986,48 @@ static void cpu_vbd_substep(CpuVBD& c, float dt, bool residual_pass) {
 // pass over the element colours (Greedy_SLF on the vertex-dual graph) with kernel_XPBD_V0
 // (GPU_PBD_FEM.cu:60-93), the constraints, then kernel_velocity_update with global damping
 // (GPU_PBD.cu:8-18).  Constraint pairs per material: eval_material (GPU_PBD_FEM_Materials.cu:97-117).
+// Rotation part of F by the quaternion iteration of Mueller et al., "A Robust Method to
+// Extract the Rotational Part of Deformations" (MIG 2016), as mat3x3_polardecomposition
+// (CUMatrix.cu:75-96) runs it: R starts at the identity, at most 10 iterations, stop when
+// |omega| < 1e-8, omega = sum_i R_i x F_i * (1/|sum_i R_i . F_i| + 1e-9); S = R^T F.
+template <class T> void polar(const M3<T>& F, M3<T>& R, M3<T>& S) {
+    T qw = 1, qx = 0, qy = 0, qz = 0;
+    R = M3<T>(T(1));
+    for (int it = 0; it < 10; ++it) {
+        const T den = T(1) / std::fabs(dot(R[0], F[0]) + dot(R[1], F[1]) + dot(R[2], F[2])) + T(1e-9);
+        const V3<T> om = (cross(R[0], F[0]) + cross(R[1], F[1]) + cross(R[2], F[2])) * den;
+        const T w = length(om);
+        if (w < T(1e-8)) break;
+        const V3<T> a = om / w;   // dq = (cos(w/2), a sin(w/2)); q = dq q; q /= |q|
+        const T c = std::cos(w * T(0.5)), sn = std::sin(w * T(0.5));
+        const T dw = c, dx = a.x * sn, dy = a.y * sn, dz = a.z * sn;
+        const T nw = dw * qw - dx * qx - dy * qy - dz * qz;
+        const T nx = dw * qx + dx * qw + dy * qz - dz * qy;
+        const T ny = dw * qy - dx * qz + dy * qw + dz * qx;
+        const T nz = dw * qz + dx * qy - dy * qx + dz * qw;
+        const T inv = T(1) / std::sqrt(nw * nw + nx * nx + ny * ny + nz * nz);
+        qw = nw * inv; qx = nx * inv; qy = ny * inv; qz = nz * inv;
+        // rotation matrix of the unit quaternion, column-major
+        R[0] = {T(1) - T(2) * (qy * qy + qz * qz), T(2) * (qx * qy + qw * qz), T(2) * (qx * qz - qw * qy)};
+        R[1] = {T(2) * (qx * qy - qw * qz), T(1) - T(2) * (qx * qx + qz * qz), T(2) * (qy * qz + qw * qx)};
+        R[2] = {T(2) * (qx * qz + qw * qy), T(2) * (qy * qz - qw * qx), T(1) - T(2) * (qx * qx + qy * qy)};
+    }
+    S = transpose(R) * F;
+}
+
 template <class T> void xpbd_pair(int mat, int m, T lambda, T mu, const M3<T>& F, M3<T>& P, T& C) {
     const M3<T> I(T(1));
-    if (mat == Hooke) {
+    if (mat == Corotated || mat == FixedCorotated) {   // GPU_PBD_FEM_Materials.cu:67-95
+        M3<T> R, S;
+        polar(F, R, S);
+        if (mat == Corotated) {
+            if (m == 0) { C = squared_trace(S - I); P = R * (T(2) * trace(S - I) * I); }
+            else { C = squared_norm(S); P = R * (T(2) * S - I); }
+        } else {
+            if (m == 0) { const T d = det(S) - T(1); C = d * d; P = R * (T(2) * d * com(S)); }
+            else { C = T(2) * squared_norm(S); P = R * (T(4) * (S - I)); }
+        }
+    } else if (mat == Hooke) {
         if (m == 0) { const T tr = trace(T(0.5) * (transpose(F) + F) - I); C = tr * tr; P = T(2) * tr * I; }
         else { const M3<T> E = T(0.5) * (transpose(F) + F) - I; C = T(2) * squared_trace(E); P = T(4) * E; }
     } else if (mat == StVK) {
@@ -1010,6 +1049,7 @@ template <class T> struct XPBD {
     Fem<T> fem;
     State<T> s;
     T global_damping = 0;
+    int version = 2;   // XPBD_FEM_VERSION: 0 XPBD, 1 Quadrature, 2 OptiShared, 3 OptiGroup
     std::vector<std::vector<int>> by_color;   // element ids per colour, ascending
     bool first = true, has_v0 = false;
 };
@@ -1024,6 +1064,12 @@ template <class T> void xpbd_substep(XPBD<T>& x, T dt) {
         s.f[i] = V3<T>();
     }
     std::vector<V3<T>> grad(f.ne);
+    // GPU_PBD_FEM::step (:661-689): Tetra4 and version XPBD run kernel_XPBD_V0 (normalised
+    // constraint sqrt|C|, masked update); Quadrature and OptiShared run kernel_XPBD_V1/V2
+    // (:141-263: raw C, alpha = 4C/(k dt^2), beta = -2C/(S + alpha), no mask); OptiGroup
+    // launches nothing for other elements.
+    const bool v0 = f.ne == 4 || x.version == 0;
+    if (!v0 && x.version != 1 && x.version != 2) x.by_color.clear();
     for (const auto& els : x.by_color)
         for (int eid : els) {
             const int* topo = &f.topo[eid * f.ne];
@@ -1040,6 +1086,18 @@ template <class T> void xpbd_substep(XPBD<T>& x, T dt) {
                     P = P * transpose(Ji) * V;
                     C += en * V;
                     for (int i = 0; i < f.ne; ++i) grad[i] = grad[i] + P * f.dN[q * f.ne + i];
+                }
+                if (!v0) {
+                    T S = 0;
+                    for (int i = 0; i < f.ne; ++i) S += dot(grad[i], grad[i]) * s.w[topo[i]];
+                    const T k = m == 0 ? f.lambda[eid] : f.mu[eid];
+                    const T alpha = T(4) * C / (k * dt * dt);
+                    const T beta = C < T(1e-12) ? T(0) : -T(2) * C / (S + alpha);
+                    for (int i = 0; i < f.ne; ++i) {
+                        const int vid = topo[i];
+                        s.p[vid] = s.p[vid] + beta * s.w[vid] * grad[i];
+                    }
+                    continue;
                 }
                 C = C < T(0) ? -C : C;   // xpbd_convert_to_constraint (:49-58)
                 C = std::sqrt(C);
@@ -1140,6 +1198,7 @@ template <class T> XPBD<T>* xpbd_create_t(const orc_desc* d) {
     if (!build_fem(d, x->fem)) { delete x; return nullptr; }
     init_state(d, x->s);
     x->global_damping = (T)d->global_damping;
+    x->version = d->xpbd_version;
     std::vector<int> c;
     Graph g = build_dual_vertex(x->fem.ne, d->topology, d->n_elements);
     const int nc = greedy_slf(g, c);
@@ -1171,6 +1230,34 @@ using namespace orc;
 extern "C" {
 
 int orc_elem_nodes(int e) { return nodes_of(e); }
+
+int orc_polar(const double* F9, int fp64, double* R9, double* S9) {
+    if (!F9) return -1;
+    auto run = [&](auto zero) {
+        using T = decltype(zero);
+        M3<T> F, R, S;
+        for (int j = 0; j < 3; ++j) F[j] = {(T)F9[3 * j], (T)F9[3 * j + 1], (T)F9[3 * j + 2]};
+        polar(F, R, S);
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) {
+                if (R9) R9[3 * j + i] = R[j][i];
+                if (S9) S9[3 * j + i] = S[j][i];
+            }
+    };
+    if (fp64) run(0.0); else run(0.0f);
+    return 0;
+}
+
+int orc_xpbd_pair(int material, int m, double lambda, double mu, const double* F9, double* P9, double* C) {
+    if (!F9 || material < Hooke || material > FixedCorotated || m < 0 || m > 1) return -1;
+    M3<double> F, P;
+    for (int j = 0; j < 3; ++j) F[j] = {F9[3 * j], F9[3 * j + 1], F9[3 * j + 2]};
+    double c = 0;
+    xpbd_pair(material, m, lambda, mu, F, P, c);
+    for (int j = 0; j < 3; ++j) for (int i = 0; i < 3; ++i) if (P9) P9[3 * j + i] = P[j][i];
+    if (C) *C = c;
+    return 0;
+}
 
 int orc_beam_counts(int e, int nx, int ny, int nz, int* n_nodes, int* n_elements) {
     Mesh m;
@@ -1296,7 +1383,7 @@ int orc_conflicts(int e, const int32_t* topo, int n_elem, int n_nodes, const int
 }
 
 void* orc_vbd_create(const orc_desc* d, int fp64) {
-    if (!d || !d->colors || !d->masses) return nullptr;
+    if (!d || !d->colors || !d->masses || d->material > StableNeoHooke) return nullptr;
     Handle* h = new Handle();
     h->kind = fp64 ? 1 : 0;
     h->ptr = fp64 ? (void*)vbd_create<double>(d) : (void*)vbd_create<float>(d);
@@ -1358,7 +1445,7 @@ void orc_vbd_destroy(void* hv) {
 }
 
 void* orc_cpuvbd_create(const orc_desc* d) {
-    if (!d || !d->masses) return nullptr;
+    if (!d || !d->masses || d->material > StableNeoHooke) return nullptr;
     auto* c = new CpuVBD();
     if (!build_fem(d, c->fem)) { delete c; return nullptr; }
     c->n = d->n_nodes;
@@ -1444,7 +1531,7 @@ void orc_xpbd_destroy(void* hv) {
 }
 
 void* orc_explicit_create(const orc_desc* d, int fp64) {
-    if (!d || !d->masses) return nullptr;
+    if (!d || !d->masses || d->material > StableNeoHooke) return nullptr;
     Handle* h = new Handle();
     h->kind = fp64 ? 5 : 4;
     h->ptr = fp64 ? (void*)explicit_create_t<double>(d) : (void*)explicit_create_t<float>(d);

@@ -29,7 +29,8 @@ typedef struct orc_desc {
     int32_t n_elements;
     const int32_t* topology;  /* n_elements*nodes_per_element */
     const float* masses;      /* n_nodes */
-    int32_t material;         /* Hooke=0, StVK=1, NeoHooke=2, Stable_NeoHooke=3 */
+    int32_t material;         /* Hooke=0, StVK=1, NeoHooke=2, Stable_NeoHooke=3, Corotated=4,
+                                 FixedCorotated=5 (XPBD only) */
     float young, poisson;
     const float* young_per_element; /* NULL or n_elements (per-element Young modulus) */
     float damping;
@@ -50,6 +51,7 @@ typedef struct orc_desc {
     float box_min[3], box_max[3];
     /* XPBD */
     float global_damping;
+    int32_t xpbd_version;     /* XPBD_FEM_VERSION: 0 XPBD, 1 Quadrature, 2 OptiShared, 3 OptiGroup */
 } orc_desc;
 
 int orc_elem_nodes(int element);
@@ -80,6 +82,12 @@ void orc_vbd_destroy(void* h);
 /* Rigid motion of fixation group g (GPU_Fix_Constraint axis): p = offset + com + R (X - com),
  * R column-major; works on VBD, XPBD and explicit handles. */
 int orc_set_fixation(void* h, int group, const float* offset, const float* rotation);
+
+/* Polar decomposition F = R S of mat3x3_polardecomposition (CUMatrix.cu:75-96), column-major,
+ * in float (fp64 = 0) or double; and one XPBD constraint pair (eval_material,
+ * GPU_PBD_FEM_Materials.cu:97-117) in double. */
+int orc_polar(const double* F9, int fp64, double* R9, double* S9);
+int orc_xpbd_pair(int material, int m, double lambda, double mu, const double* F9, double* P9, double* C);
 
 /* Reference CPU VBD (VertexBlockDescent.cpp + VBD_FEM.cpp): single-thread Gauss-Seidel in
  * vertex order with the per-iteration full force pass (plot_residual). */

@@ -12,7 +12,8 @@ LIB_PATH = os.path.join(ORACLE_DIR, "liboracle.so")
 
 TETRA, PYRAMID, PRISM, HEXA, TETRA10, TETRA20, HEXA27 = 3, 4, 5, 6, 7, 8, 9
 ELEMENT_NODES = {TETRA: 4, HEXA: 8, TETRA10: 10, TETRA20: 20, HEXA27: 27}
-HOOKE, STVK, NEOHOOKE, STABLE_NEOHOOKE = 0, 1, 2, 3
+HOOKE, STVK, NEOHOOKE, STABLE_NEOHOOKE, COROTATED, FIXED_COROTATED = 0, 1, 2, 3, 4, 5
+XPBD_V0, XPBD_QUADRATURE, XPBD_OPTISHARED, XPBD_OPTIGROUP = 0, 1, 2, 3
 
 
 class OrcDesc(C.Structure):
@@ -26,7 +27,7 @@ class OrcDesc(C.Structure):
         ("iterations", C.c_int32), ("rho", C.c_float), ("in_place", C.c_int32), ("n_colors", C.c_int32),
         ("colors", C.POINTER(C.c_int32)), ("order_mode", C.c_int32), ("seed", C.c_uint64),
         ("box_limit", C.c_int32), ("box_min", C.c_float * 3), ("box_max", C.c_float * 3),
-        ("global_damping", C.c_float),
+        ("global_damping", C.c_float), ("xpbd_version", C.c_int32),
     ]
 
 
@@ -64,12 +65,31 @@ def lib():
         L.orc_cpuvbd_destroy.argtypes = [vp]
         L.orc_cpuvbd_run_many.argtypes = [C.POINTER(vp), C.c_int, C.c_float, C.c_int, C.c_int, C.c_int]
         L.orc_cpuvbd_run_many.restype = C.c_double
+        L.orc_polar.argtypes = [dp, C.c_int, dp, dp]
+        L.orc_xpbd_pair.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, dp, dp, dp]
         _lib = L
     return _lib
 
 
 def _p(a, t):
     return a.ctypes.data_as(C.POINTER(t)) if a is not None else None
+
+
+def polar(F, fp64=True):
+    """(R, S) of the reference polar decomposition of a 3x3 matrix (row-major numpy in and out)."""
+    Fc = np.ascontiguousarray(np.asarray(F, np.float64).T)   # column-major
+    R, S = np.zeros(9), np.zeros(9)
+    lib().orc_polar(_p(Fc.ravel(), C.c_double), int(fp64), _p(R, C.c_double), _p(S, C.c_double))
+    return R.reshape(3, 3).T, S.reshape(3, 3).T
+
+
+def xpbd_pair(material, m, lam, mu, F):
+    """(P, C) of one XPBD constraint of eval_material (row-major numpy in and out)."""
+    Fc = np.ascontiguousarray(np.asarray(F, np.float64).T)
+    P, c = np.zeros(9), C.c_double()
+    rc = lib().orc_xpbd_pair(material, m, lam, mu, _p(Fc.ravel(), C.c_double), _p(P, C.c_double), C.byref(c))
+    assert rc == 0
+    return P.reshape(3, 3).T, c.value
 
 
 def beam_mesh(element, cells, size, offset=(0.0, 0.0, 0.0)):
@@ -138,7 +158,7 @@ class Scene:
     def __init__(self, element, X, T, m, material=STABLE_NEOHOOKE, young=1e5, poisson=0.45, damping=0.0,
                  gravity=(0, 0, -9.81), fixed=(), v0=None, iterations=20, rho=0.0, in_place=False, colors=None,
                  n_colors=0, order_mode=0, seed=0, young_per_element=None, box=None, global_damping=0.0,
-                 fixed_group=None):
+                 fixed_group=None, xpbd_version=2):
         self.arrays = dict(X=np.ascontiguousarray(X, np.float32), T=np.ascontiguousarray(T, np.int32),
                            m=np.ascontiguousarray(m, np.float32), fixed=np.ascontiguousarray(fixed, np.int32),
                            v0=None if v0 is None else np.ascontiguousarray(v0, np.float32),
@@ -175,6 +195,7 @@ class Scene:
             d.box_min = (C.c_float * 3)(*box[0])
             d.box_max = (C.c_float * 3)(*box[1])
         d.global_damping = global_damping
+        d.xpbd_version = xpbd_version
         self.desc = d
         self.n = d.n_nodes
 

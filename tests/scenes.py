@@ -16,7 +16,7 @@ def make_mesh(element, cells, size, offset=(0.0, 0.0, 0.0)):
 def pair(ctx, element, cells=(4, 2, 2), size=(1.0, 0.25, 0.25), material=O.STABLE_NEOHOOKE, young=1e5,
          poisson=0.45, density=1000.0, gravity=(0.0, 0.0, -9.81), iterations=10, damping=0.0, v0=None,
          solver="vbd", precision=0, tpv=0, version=2, target=-1, rho=0.0, young_per_element=None, box=None,
-         global_damping=0.0, color_algo=0, fixed=None):
+         global_damping=0.0, color_algo=0, fixed=None, xpbd_version=2):
     """Returns (product Scene, oracle fp32 solver, oracle fp64 solver, mesh dict)."""
     import octopusengine_b200 as ob
     X, T = make_mesh(element, cells, size)
@@ -27,7 +27,7 @@ def pair(ctx, element, cells=(4, 2, 2), size=(1.0, 0.25, 0.25), material=O.STABL
     kw = dict(solver=kind, masses=m, material=material, young=young, poisson=poisson, damping=damping,
               gravity=gravity, fixed_ids=fixed, iterations=iterations, precision=precision,
               threads_per_vertex=tpv, vbd_version=version, target_color=target, rho=rho, color_algo=color_algo,
-              global_damping=global_damping)
+              global_damping=global_damping, xpbd_version=xpbd_version)
     if v0 is not None:
         kw["initial_velocity"] = v0
     if young_per_element is not None:
@@ -42,7 +42,7 @@ def pair(ctx, element, cells=(4, 2, 2), size=(1.0, 0.25, 0.25), material=O.STABL
         in_place = O.conflicts(element, T, len(X), colors) == 0
     okw = dict(material=material, young=young, poisson=poisson, damping=damping, gravity=gravity, fixed=fixed,
                v0=v0, iterations=iterations, rho=rho, in_place=in_place, colors=colors, n_colors=n_colors,
-               young_per_element=young_per_element, box=box, global_damping=global_damping)
+               young_per_element=young_per_element, box=box, global_damping=global_damping, xpbd_version=xpbd_version)
     s32 = O.Scene(element, X, T, m, **okw)
     s64 = O.Scene(element, X, T, m, **okw)
     o32 = O.Solver(solver, s32, fp64=False)
