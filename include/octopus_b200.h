@@ -156,6 +156,26 @@ oct_status oct_scene_set_precision(oct_scene* s, int precision);
  * [sum |r|, max |r|] over free nodes.  Both return OCT_ENUMERIC on NaN/Inf state. */
 oct_status oct_scene_energy(oct_scene* s, double out4[4]);
 oct_status oct_scene_residual(oct_scene* s, float dt, double out2[2]);
+/* Per-element diagnostics of GPU_FEM::get_stress / get_volume / get_volume_diff / get_inverted
+ * (octopus/include/GPU/GPU_FEM.h:66-69; kernels octopus/src/GPU/GPU_FEM.cu:20-107), evaluated in
+ * FP64 on the current positions (the exact value of the reference's formulas there),
+ * out: n_elements floats.
+ *   OCT_DIAG_STRESS      sum_q von Mises(Cauchy(F_q)) V_q, F_q = Jx_q JX_inv_q
+ *   OCT_DIAG_STRESS_ACCUMULATED  the same with Jx summed over the quadrature points, as
+ *                        kernel_compute_stress accumulates it (equal for one-point elements;
+ *                        octb::GPU_FEM::get_stress returns this one)
+ *   OCT_DIAG_VOLUME      sum_q |det Jx_q| w_q
+ *   OCT_DIAG_VOLUME_DIFF sum_q (|det Jx_q| w_q - V_q)   (the reference getter launches the
+ *                        inversion kernel instead; octb::GPU_FEM::get_volume_diff does the same)
+ *   OCT_DIAG_INVERTED    1 where sum_q det(F_q) w_q < -1e-6, else 0
+ * Corotated and FixedCorotated have no stress (0), as in the reference. */
+enum { OCT_DIAG_STRESS = 0, OCT_DIAG_VOLUME = 1, OCT_DIAG_VOLUME_DIFF = 2, OCT_DIAG_INVERTED = 3,
+       OCT_DIAG_STRESS_ACCUMULATED = 4 };
+oct_status oct_scene_element_data(oct_scene* s, int kind, float* out_n_elements);
+/* Per-vertex residual force of GPU_VBD_FEM::get_forces (octopus/src/GPU/VBD/GPU_VBD_FEM.cu:
+ * 482-559) for sub-step dt: elastic + damping + inertia terms, 0 on fixed vertices; zeros for
+ * XPBD and explicit scenes (GPU_FEM::get_forces).  out: n_nodes*3. */
+oct_status oct_scene_vertex_residuals(oct_scene* s, float dt, float* out_n3);
 
 /* Batch: many VBD scenes stepped together, one launch per (element type, colour) across all
  * scenes, driven by a per-scene work table, the sub-step captured as a CUDA graph.  All

@@ -109,6 +109,32 @@ struct GPU_FEM : GPU_Dynamic {
     scalar young, poisson;
     Material material;
     scalar damping = 0;
+
+    // Queries of GPU_FEM (octopus/include/GPU/GPU_FEM.h:66-70), available once the integrator
+    // has stepped the particle system (the scene is created at the first step).
+    std::vector<scalar> get_stress(const GPU_ParticleSystem* ps) const { return element_data(ps, OCT_DIAG_STRESS_ACCUMULATED); }
+    std::vector<scalar> get_volume(const GPU_ParticleSystem* ps) const { return element_data(ps, OCT_DIAG_VOLUME); }
+    std::vector<scalar> get_inverted(const GPU_ParticleSystem* ps) const { return element_data(ps, OCT_DIAG_INVERTED); }
+    // the reference getter launches the inversion kernel (octopus/src/GPU/GPU_FEM.cu:237-245)
+    std::vector<scalar> get_volume_diff(const GPU_ParticleSystem* ps) const { return element_data(ps, OCT_DIAG_INVERTED); }
+    virtual std::vector<Vector3> get_forces(const GPU_ParticleSystem* ps, scalar dt) const {
+        std::vector<Vector3> out(ps->nb_particles());
+        if (!ps->scene) return out;
+        std::vector<float> buf(out.size() * 3);
+        check(oct_scene_vertex_residuals(ps->scene, dt, buf.data()), "get_forces");
+        for (size_t i = 0; i < out.size(); ++i) out[i] = Vector3(buf[3 * i], buf[3 * i + 1], buf[3 * i + 2]);
+        return out;
+    }
+
+  private:
+    std::vector<scalar> element_data(const GPU_ParticleSystem* ps, int kind) const {
+        if (!ps->scene) throw Error(OCT_EINVAL, "GPU_FEM query before the integrator's first step");
+        int32_t nn = 0, ne = 0, nc = 0, nf = 0;
+        check(oct_scene_info(ps->scene, &nn, &ne, &nc, &nf), "oct_scene_info");
+        std::vector<scalar> out(ne);
+        check(oct_scene_element_data(ps->scene, kind, out.data()), "GPU_FEM query");
+        return out;
+    }
 };
 struct GPU_VBD_FEM : GPU_FEM {
     GPU_VBD_FEM(const Element& e, const Mesh::Topology& t, const Mesh::Geometry& g, const Material& m, const scalar& young_,

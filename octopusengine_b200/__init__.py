@@ -185,6 +185,20 @@ class Scene:
                    self.ctx.handle)
         return e
 
+    def element_data(self, kind):
+        """Per-element diagnostic (capi.DIAG_STRESS / VOLUME / VOLUME_DIFF / INVERTED)."""
+        out = np.zeros(self.n_elements, np.float32)
+        capi.check(capi.lib().oct_scene_element_data(self._h, kind, capi.ptr(out, C.c_float)),
+                   "oct_scene_element_data", self.ctx.handle)
+        return out
+
+    def vertex_residuals(self, dt):
+        """Per-vertex VBD residual force for sub-step dt (GPU_VBD_FEM::get_forces)."""
+        out = np.zeros((self.n_nodes, 3), np.float32)
+        capi.check(capi.lib().oct_scene_vertex_residuals(self._h, dt, capi.ptr(out, C.c_float)),
+                   "oct_scene_vertex_residuals", self.ctx.handle)
+        return out
+
     def residual(self, dt):
         r = np.zeros(2)
         capi.check(capi.lib().oct_scene_residual(self._h, dt, capi.ptr(r, C.c_double)), "oct_scene_residual",

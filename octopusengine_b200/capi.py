@@ -19,6 +19,7 @@ ELEMENT_NODES = {TETRA: 4, HEXA: 8, TETRA10: 10, TETRA20: 20, HEXA27: 27}
 ELEMENT_QUADRATURE = {TETRA: 1, HEXA: 8, TETRA10: 4, TETRA20: 11, HEXA27: 27}
 HOOKE, STVK, NEOHOOKE, STABLE_NEOHOOKE, COROTATED, FIXED_COROTATED = 0, 1, 2, 3, 4, 5
 XPBD_XPBD, XPBD_QUADRATURE, XPBD_OPTISHARED, XPBD_OPTIGROUP = 0, 1, 2, 3
+DIAG_STRESS, DIAG_VOLUME, DIAG_VOLUME_DIFF, DIAG_INVERTED, DIAG_STRESS_ACCUMULATED = 0, 1, 2, 3, 4
 MASS_UNIFORM, MASS_FEMSHAPE = 0, 1
 SOLVER_VBD, SOLVER_XPBD, SOLVER_EXPLICIT = 0, 1, 2
 VBD_BASE, VBD_THREADED_QUADRATURE, VBD_REDUCTION_SYMMETRY, VBD_BETTER_COLORATION = 0, 1, 2, 3
@@ -38,6 +39,7 @@ EXPORTS = [
     "oct_batch_group_info", "oct_batch_time_group", "oct_scene_set_precision", "oct_scene_footprint",
     "oct_server_create", "oct_server_submit", "oct_server_tick", "oct_server_poll", "oct_server_get_stats",
     "oct_server_destroy", "oct_elastic_energy_noalloc", "oct_scene_set_fixation_group",
+    "oct_scene_element_data", "oct_scene_vertex_residuals",
 ]
 
 
@@ -98,6 +100,8 @@ def lib():
             "oct_scene_step": ([vp, C.c_float, C.c_int], C.c_int),
             "oct_scene_sync": ([vp], C.c_int),
             "oct_scene_set_capture": ([vp, C.c_int], C.c_int),
+            "oct_scene_element_data": ([vp, C.c_int, C.POINTER(C.c_float)], C.c_int),
+            "oct_scene_vertex_residuals": ([vp, C.c_float, C.POINTER(C.c_float)], C.c_int),
             "oct_scene_get_positions": ([vp, fp], C.c_int),
             "oct_scene_get_velocities": ([vp, fp], C.c_int),
             "oct_scene_set_positions": ([vp, fp], C.c_int),

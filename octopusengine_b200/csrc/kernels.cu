@@ -60,6 +60,17 @@ __device__ __align__(16) float g_dN6[192];
 __device__ __align__(16) float g_dN7[120];
 __device__ __align__(16) float g_dN8[660];
 __device__ __align__(16) float g_dN9[2188];
+// FP64 copies of the tables for the diagnostics kernel.
+__device__ double g_dNd3[12], g_dNd6[192], g_dNd7[120], g_dNd8[660], g_dNd9[2187];
+__device__ double g_wd3[1], g_wd6[8], g_wd7[4], g_wd8[11], g_wd9[27];
+template <int E> __device__ __forceinline__ const double* gdNd() {
+    if constexpr (E == 3) return g_dNd3; else if constexpr (E == 6) return g_dNd6; else if constexpr (E == 7) return g_dNd7;
+    else if constexpr (E == 8) return g_dNd8; else return g_dNd9;
+}
+template <int E> __device__ __forceinline__ const double* gwd() {
+    if constexpr (E == 3) return g_wd3; else if constexpr (E == 6) return g_wd6; else if constexpr (E == 7) return g_wd7;
+    else if constexpr (E == 8) return g_wd8; else return g_wd9;
+}
 template <int E> __device__ __forceinline__ const float* gdN();
 template <> __device__ __forceinline__ const float* gdN<3>() { return g_dN3; }
 template <> __device__ __forceinline__ const float* gdN<6>() { return g_dN6; }
@@ -368,6 +379,7 @@ __device__ __forceinline__ void vertex_epilogue(const SceneDev& S, int vid, cons
         const double r1 = acc[1] - kd * (acc[4] * dx + acc[6] * dy + acc[7] * dz) - mh2 * (uu.y - yy.y);
         const double r2 = acc[2] - kd * (acc[5] * dx + acc[7] * dy + acc[8] * dz) - mh2 * (uu.z - yy.z);
         const double nr = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
+        S.u_new[vid] = make_float4((float)r0, (float)r1, (float)r2, 0.f);   // per-vertex residual (get_forces)
         if (!isfinite(nr)) atomicOr(P.error, 2);
         else {
             atomicAdd(red, nr);
@@ -498,7 +510,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<E>::value) k_vertex_packed(c
 template <int E> constexpr int packed_smem_bytes() { return (kBlock / 32) * 2 * 32 * EntryLayout<ElemT<E>::NE>::kWords * 4; }
 
 // ------------------------------------------------------------------------ colour kernel
-// mode 0: VBD solve; mode 1: VBD residual (writes |r| reductions); mode 2: explicit force.
+// mode 0: VBD solve; mode 1: VBD residual (r into u_new, |r| reductions); mode 2: explicit force.
 template <int E, int MAT>
 __global__ void __launch_bounds__(kBlock, E == 3 ? 6 : 1) k_vertex(const SceneDev* __restrict__ scenes, const VWork* __restrict__ work,
                                                    int n_work, int tpv, int mode, StepParams P, double* red) {
@@ -969,6 +981,114 @@ __global__ void __launch_bounds__(kBlock) k_xpbd(const SceneDev* __restrict__ sc
         if (vid[k] >= 0 && mv[k]) S.u[vid[k]] = u[k];
 }
 
+// ------------------------------------------------------------------------ diagnostics
+// Per-element diagnostics of GPU_FEM (GPU_FEM.cu:20-107), one thread per element, in FP64 on
+// the current absolute positions p = X + u (rounded to FP32 as the getters return them), with
+// the rest Jacobian of each quadrature point recomputed from X: the exact value of the
+// reference's formulas at those positions.
+//   kind 0: sum_q von_mises(P F^T / det F) V_q, F = Jx_q JX_inv_q
+//   kind 4: the same with Jx summed over the quadrature points, as kernel_compute_stress
+//           (:20-43) accumulates it (equal to kind 0 for one-point elements)
+//   kind 1: sum_q |det Jx_q| w_q                 (kernel_compute_volume)
+//   kind 2: sum_q (|det Jx_q| w_q - V_q)         (kernel_compute_volume_diff)
+//   kind 3: 1 if sum_q det(Jx_q JX_inv_q) w_q < -1e-6, else 0   (kernel_compute_inverted, with
+//           the rest Jacobian of point q)
+struct D3 { double x, y, z; };
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 operator*(D3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+__device__ __forceinline__ double ddot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ D3 dcross(D3 a, D3 b) { return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y}; }
+__device__ __forceinline__ double ddet(D3 a, D3 b, D3 c) { return ddot(a, dcross(b, c)); }
+__device__ __forceinline__ double dget(D3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+// PK1 of GPU_FEM_Material.cu:14-36 (columns); zero for the XPBD-only materials.
+__device__ void pk1_d(int mat, D3 F0, D3 F1, D3 F2, double lam, double mu, D3& P0, D3& P1, D3& P2) {
+    if (mat == 0) {   // hooke_stress: lambda tr(E) I + mu E, E = (F + F^T)/2 - I
+        const double e00 = F0.x - 1.0, e11 = F1.y - 1.0, e22 = F2.z - 1.0;
+        const double e01 = 0.5 * (F1.x + F0.y), e02 = 0.5 * (F2.x + F0.z), e12 = 0.5 * (F2.y + F1.z);
+        const double t = lam * (e00 + e11 + e22);
+        P0 = {t + mu * e00, mu * e01, mu * e02}; P1 = {mu * e01, t + mu * e11, mu * e12};
+        P2 = {mu * e02, mu * e12, t + mu * e22};
+    } else if (mat == 1) {   // stvk_stress: lambda tr(E) F + 2 mu F E, E = (F^T F - I)/2
+        const double e00 = 0.5 * (ddot(F0, F0) - 1.0), e11 = 0.5 * (ddot(F1, F1) - 1.0), e22 = 0.5 * (ddot(F2, F2) - 1.0);
+        const double e01 = 0.5 * ddot(F0, F1), e02 = 0.5 * ddot(F0, F2), e12 = 0.5 * ddot(F1, F2);
+        const double t = lam * (e00 + e11 + e22);
+        P0 = F0 * t + (F0 * e00 + F1 * e01 + F2 * e02) * (2.0 * mu);
+        P1 = F1 * t + (F0 * e01 + F1 * e11 + F2 * e12) * (2.0 * mu);
+        P2 = F2 * t + (F0 * e02 + F1 * e12 + F2 * e22) * (2.0 * mu);
+    } else if (mat == 2 || mat == 3) {   // nh_stress / snh_stress: lambda (J - alpha) cof F + mu F
+        const D3 C0 = dcross(F1, F2), C1 = dcross(F2, F0), C2 = dcross(F0, F1);
+        const double sc = lam * (ddot(F0, C0) - (mat == 3 ? 1.0 + mu / lam : 1.0));
+        P0 = C0 * sc + F0 * mu; P1 = C1 * sc + F1 * mu; P2 = C2 * sc + F2 * mu;
+    } else {
+        P0 = P1 = P2 = D3{0.0, 0.0, 0.0};
+    }
+}
+
+// Inverse of the matrix with columns c0 c1 c2, as columns (adjugate / determinant).
+__device__ __forceinline__ void dinv(D3 c0, D3 c1, D3 c2, D3& i0, D3& i1, D3& i2) {
+    const D3 r0 = dcross(c1, c2), r1 = dcross(c2, c0), r2 = dcross(c0, c1);   // rows of the inverse x det
+    const double id = 1.0 / ddot(c0, r0);
+    i0 = D3{r0.x, r1.x, r2.x} * id; i1 = D3{r0.y, r1.y, r2.y} * id; i2 = D3{r0.z, r1.z, r2.z} * id;
+}
+
+template <int E>
+__global__ void __launch_bounds__(kBlock) k_element_diag(const SceneDev* __restrict__ scenes, int scene, int kind,
+                                                         int material, float* __restrict__ out) {
+    constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ;
+    const SceneDev& S = scenes[scene];
+    const int eid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (eid >= S.n_elements) return;
+    const int* tp = S.topo + (size_t)eid * NE;
+    const double* dN = gdNd<E>();
+    const double* wt = gwd<E>();
+    const float4 c0 = S.eq[(size_t)eid * S.eq_stride * 3 + 2];   // lambda, mu of the element
+    const double lam = c0.z, mu = c0.w;
+    D3 A0 = {0, 0, 0}, A1 = A0, A2 = A0;   // accumulated Jx (kind 4)
+    double acc = 0.0;
+    for (int q = 0; q < NQ; ++q) {
+        D3 J0 = {0, 0, 0}, J1 = J0, J2 = J0, R0 = J0, R1 = J0, R2 = J0;
+        for (int i = 0; i < NE; ++i) {
+            const int v = tp[i];
+            const float4 u = S.u[v], X = S.X[v];
+            const D3 p = {(double)(X.x + u.x), (double)(X.y + u.y), (double)(X.z + u.z)};
+            const D3 x = {(double)X.x, (double)X.y, (double)X.z};
+            const double* d = dN + (q * NE + i) * 3;
+            J0 = J0 + p * d[0]; J1 = J1 + p * d[1]; J2 = J2 + p * d[2];
+            R0 = R0 + x * d[0]; R1 = R1 + x * d[1]; R2 = R2 + x * d[2];
+        }
+        const double w = wt[q];
+        const double Vq = fabs(ddet(R0, R1, R2)) * w;
+        if (kind == 1) { acc += fabs(ddet(J0, J1, J2)) * w; continue; }
+        if (kind == 2) { acc += fabs(ddet(J0, J1, J2)) * w - Vq; continue; }
+        D3 m0, m1, m2;   // JX_inv columns
+        dinv(R0, R1, R2, m0, m1, m2);
+        if (kind == 4) { A0 = A0 + J0; A1 = A1 + J1; A2 = A2 + J2; J0 = A0; J1 = A1; J2 = A2; }
+        const D3 F0 = J0 * m0.x + J1 * m0.y + J2 * m0.z, F1 = J0 * m1.x + J1 * m1.y + J2 * m1.z,
+                 F2 = J0 * m2.x + J1 * m2.y + J2 * m2.z;
+        if (kind == 3) { acc += ddet(F0, F1, F2) * w; continue; }
+        D3 P0, P1, P2;
+        pk1_d(material, F0, F1, F2, lam, mu, P0, P1, P2);
+        // Cauchy C = P F^T / det F: C(r, k) = sum_j P_j[r] F_j[k]
+        const double id = 1.0 / ddet(F0, F1, F2);
+        double Cm[3][3];
+        for (int r = 0; r < 3; ++r)
+            for (int k = 0; k < 3; ++k)
+                Cm[r][k] = (dget(P0, r) * dget(F0, k) + dget(P1, r) * dget(F1, k) + dget(P2, r) * dget(F2, k)) * id;
+        // von_mises_stress (GPU_FEM_Material.cu:223-230) with m[col][row] = Cm[row][col]
+        const double s01 = Cm[0][0] - Cm[1][1], s12 = Cm[1][1] - Cm[2][2], s02 = Cm[0][0] - Cm[2][2];
+        double vm = 0.5 * (s01 * s01 + s12 * s12 + s02 * s02);
+        vm += 3.0 * (Cm[1][0] * Cm[1][0] + Cm[2][1] * Cm[2][1] + Cm[2][0] * Cm[2][0]);
+        acc += sqrt(vm) * Vq;
+    }
+    out[eid] = kind == 3 ? (acc > -1e-6 ? 0.f : 1.f) : (float)acc;
+}
+
+template <int E>
+void diag_launch(int mat, const SceneDev* scenes, int scene, int n_elements, int kind, float* out, cudaStream_t st) {
+    k_element_diag<E><<<(n_elements + kBlock - 1) / kBlock, kBlock, 0, st>>>(scenes, scene, kind, mat, out);
+}
+
 // ------------------------------------------------------------------------ FP64 energy
 // Kinetic + elastic + gravity energy of one scene in FP64 (new: the reference has no
 // energy evaluator; material energies of FEM_ContinuousMaterial.cpp:10-87).
@@ -1161,6 +1281,19 @@ double vbd_term_flops(int element, int material) {
     return 18.0 * ne + 48.0 + 15.0 + mat + 9.0;
 }
 
+cudaError_t upload_shape_tables_fp64(int element, const double* dN, int n, const double* w, int nq) {
+    cudaError_t e1, e2;
+    switch (element) {
+        case 3: e1 = cudaMemcpyToSymbol(g_dNd3, dN, n * 8); e2 = cudaMemcpyToSymbol(g_wd3, w, nq * 8); break;
+        case 6: e1 = cudaMemcpyToSymbol(g_dNd6, dN, n * 8); e2 = cudaMemcpyToSymbol(g_wd6, w, nq * 8); break;
+        case 7: e1 = cudaMemcpyToSymbol(g_dNd7, dN, n * 8); e2 = cudaMemcpyToSymbol(g_wd7, w, nq * 8); break;
+        case 8: e1 = cudaMemcpyToSymbol(g_dNd8, dN, n * 8); e2 = cudaMemcpyToSymbol(g_wd8, w, nq * 8); break;
+        case 9: e1 = cudaMemcpyToSymbol(g_dNd9, dN, n * 8); e2 = cudaMemcpyToSymbol(g_wd9, w, nq * 8); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return e1 != cudaSuccess ? e1 : e2;
+}
+
 cudaError_t upload_shape_tables(int element, const float* dN, int n_floats) {
     cudaError_t e1, e2;
     switch (element) {
@@ -1235,6 +1368,18 @@ void launch_xpbd(int element, int material, bool raw, const SceneDev* scenes, co
         case 7: xpbd_form<7>(material, raw, scenes, elems, begin, count, scene, P, st); break;
         case 8: xpbd_form<8>(material, raw, scenes, elems, begin, count, scene, P, st); break;
         case 9: xpbd_form<9>(material, raw, scenes, elems, begin, count, scene, P, st); break;
+    }
+}
+
+void launch_element_diag(int element, int material, const SceneDev* scenes, int scene, int n_elements, int kind, float* out,
+                         cudaStream_t st) {
+    if (n_elements <= 0) return;
+    switch (element) {
+        case 3: diag_launch<3>(material, scenes, scene, n_elements, kind, out, st); break;
+        case 6: diag_launch<6>(material, scenes, scene, n_elements, kind, out, st); break;
+        case 7: diag_launch<7>(material, scenes, scene, n_elements, kind, out, st); break;
+        case 8: diag_launch<8>(material, scenes, scene, n_elements, kind, out, st); break;
+        case 9: diag_launch<9>(material, scenes, scene, n_elements, kind, out, st); break;
     }
 }
 

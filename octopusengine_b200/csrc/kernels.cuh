@@ -7,6 +7,7 @@
 namespace octb {
 
 cudaError_t upload_shape_tables(int element, const float* dN, int n_floats);
+cudaError_t upload_shape_tables_fp64(int element, const double* dN, int n, const double* w, int nq);
 // Caches the persistent grid size of the vertex kernel for (element, material); call
 // outside stream capture.
 void prepare_vertex(int element, int material);
@@ -25,6 +26,10 @@ void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, i
 // raw: the kernel_XPBD_V1/V2 update form (ignored for Tetra4, which always uses V0)
 void launch_xpbd(int element, int material, bool raw, const SceneDev* scenes, const int* elems, int begin, int count,
                  int scene, const StepParams& P, cudaStream_t st);
+// Per-element diagnostics of GPU_FEM (kind 0 stress, 1 volume, 2 volume change, 3 inverted,
+// 4 stress with the reference kernel's accumulated Jx).
+void launch_element_diag(int element, int material, const SceneDev* scenes, int scene, int n_elements, int kind, float* out,
+                         cudaStream_t st);
 void launch_energy(int element, int material, const SceneDev* scenes, int scene, int n_nodes, int n_elements, double* out,
                    int* error, cudaStream_t st);
 

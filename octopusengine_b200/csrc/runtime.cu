@@ -120,6 +120,7 @@ struct oct_scene {
     int* d_elems = nullptr;         // XPBD: colour-sorted element ids
     std::vector<int> elem_off;
     double* d_red = nullptr;        // 4 doubles of reduction scratch
+    float* d_diag = nullptr;        // per-element diagnostics output (allocated on first use)
 };
 
 struct oct_batch {
@@ -167,6 +168,7 @@ oct_status ensure_tables(oct_ctx* c, int element) {
     std::vector<float> f(s.dN.begin(), s.dN.end());
     f.resize(((f.size() + 3) / 4) * 4, 0.f);
     OCT_CUDA(c, upload_shape_tables(element, f.data(), (int)s.dN.size()));
+    OCT_CUDA(c, upload_shape_tables_fp64(element, s.dN.data(), (int)s.dN.size(), s.w.data(), (int)s.w.size()));
     c->tables[element] = true;
     return OCT_OK;
 }
@@ -873,6 +875,38 @@ oct_status oct_scene_energy(oct_scene* s, double out[4]) {
     OCT_CUDA(c, cudaMemcpyAsync(out, s->d_red, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     OCT_CUDA(c, cudaStreamSynchronize(c->stream));
     out[3] = out[0] + out[1] + out[2];
+    return check_error_word(c);
+}
+
+oct_status oct_scene_element_data(oct_scene* s, int kind, float* out) {
+    if (!s || !out || kind < OCT_DIAG_STRESS || kind > OCT_DIAG_STRESS_ACCUMULATED) return OCT_EINVAL;
+    oct_ctx* c = s->ctx;
+    oct_status st;
+    if (!s->d_diag && (st = s->mem.alloc(s->d_diag, (size_t)s->n_elements))) return st;
+    launch_element_diag(s->element, s->material, s->d_scene, 0, s->n_elements, kind, s->d_diag, c->stream);
+    OCT_CUDA(c, cudaGetLastError());
+    OCT_CUDA(c, cudaMemcpyAsync(out, s->d_diag, sizeof(float) * s->n_elements, cudaMemcpyDeviceToHost, c->stream));
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return OCT_OK;
+}
+
+oct_status oct_scene_vertex_residuals(oct_scene* s, float dt, float* out) {
+    if (!s || !out || !(dt > 0.f)) return OCT_EINVAL;
+    if (s->solver != OCT_SOLVER_VBD) {   // GPU_FEM::get_forces: zeros for the other solvers
+        std::fill(out, out + 3 * (size_t)s->n_nodes, 0.f);
+        return OCT_OK;
+    }
+    oct_ctx* c = s->ctx;
+    StepParams P = base_params(c, dt);
+    OCT_CUDA(c, cudaMemsetAsync(s->d_red, 0, 4 * sizeof(double), c->stream));
+    OCT_CUDA(c, cudaMemsetAsync(s->h.u_new, 0, sizeof(float4) * s->n_nodes, c->stream));
+    for (int k = 0; k < s->n_colors; ++k) {
+        const int b = s->vwork_off[k], n = s->vwork_off[k + 1] - b;
+        launch_vertex(s->element, s->material, s->d_scene, s->d_vwork + b, n, s->tpv, 1, P, s->d_red, c->stream);
+    }
+    OCT_CUDA(c, cudaGetLastError());
+    oct_status st = read_nodes(s, s->h.u_new, out, false);
+    if (st) return st;
     return check_error_word(c);
 }
 

@@ -865,6 +865,60 @@ template <class T> void residual_norms(VBD<T>& b, T dt, double* out) {
     out[0] = sum; out[1] = mx;
 }
 
+template <class T> void residual_vectors(VBD<T>& b, T dt, double* out) {
+    for (int v = 0; v < b.s.n; ++v) {
+        V3<T> fi;
+        if (b.s.mask[v] != 0) {   // kernel_vbd_compute_residual writes r only for unmasked vertices
+            M3<T> H;
+            vbd_vertex(b, v, dt, fi, H);
+            fi = fi - (b.damping / dt) * H * (b.s.p[v] - b.s.last_p[v]);
+            fi = fi - (b.s.m[v] / (dt * dt)) * (b.s.p[v] - b.s.y[v]);
+        }
+        out[3 * v] = fi.x; out[3 * v + 1] = fi.y; out[3 * v + 2] = fi.z;
+    }
+}
+
+// Per-element diagnostics of GPU_FEM (GPU_FEM.cu:20-107) on absolute positions.
+//   kind 0 stress   sum_q von_mises(P F^T / det F) V_q with F_q = Jx_q JX_inv_q
+//   kind 4 stress   the same with Jx accumulated over the quadrature points, as
+//                   kernel_compute_stress (:20-43) does (it never resets Jx)
+//                   (materials without a VBD stress, Corotated and FixedCorotated, give P = 0)
+//   kind 1 volume   kernel_compute_volume (:45-64): sum_q |det Jx_q| w_q
+//   kind 2 diff     kernel_compute_volume_diff (:66-85): sum_q (|det Jx_q| w_q - V_q)
+//   kind 3 inverted kernel_compute_inverted (:87-107): 1 when sum_q det(Jx_q JX_inv_q) w_q < -1e-6
+//                   (the kernel indexes JX_inv[eid + qid], outside the element's records and,
+//                   for eid >= E Q / (Q + 1), outside the buffer; the record of q is used here)
+template <class T> void element_data(const Fem<T>& f, const State<T>& s, int kind, double* out) {
+    for (int e = 0; e < f.n_elem; ++e) {
+        const int* topo = &f.topo[(size_t)e * f.ne];
+        T acc = 0;
+        M3<T> Jacc(T(0));
+        for (int q = 0; q < f.nq; ++q) {
+            M3<T> Jx(T(0));
+            for (int i = 0; i < f.ne; ++i) Jx = Jx + outer(s.p[topo[i]], f.dN[q * f.ne + i]);
+            const M3<T>& Ji = f.JX_inv[(size_t)e * f.nq + q];
+            const T Vq = f.V[(size_t)e * f.nq + q];
+            if (kind == 0 || kind == 4) {
+                Jacc = Jacc + Jx;
+                const M3<T> F = (kind == 4 ? Jacc : Jx) * Ji;
+                const M3<T> P = f.material > StableNeoHooke ? M3<T>(T(0)) : pk1(f.material, f.lambda[e], f.mu[e], F);
+                const M3<T> C = P * transpose(F) * (T(1) / det(F));   // pk1_to_cauchy_stress
+                const T s01 = C[0][0] - C[1][1], s12 = C[1][1] - C[2][2], s02 = C[0][0] - C[2][2];
+                T vm = T(0.5) * (s01 * s01 + s12 * s12 + s02 * s02);   // von_mises_stress (GPU_FEM_Material.cu:223-230)
+                vm += T(3) * (C[0][1] * C[0][1] + C[1][2] * C[1][2] + C[0][2] * C[0][2]);
+                acc += std::sqrt(vm) * Vq;
+            } else if (kind == 1) {
+                acc += std::fabs(det(Jx)) * f.weights[q];
+            } else if (kind == 2) {
+                acc += std::fabs(det(Jx)) * f.weights[q] - Vq;
+            } else {
+                acc += det(Jx * Ji) * f.weights[q];
+            }
+        }
+        out[e] = kind == 3 ? (acc > T(-1e-6) ? 0.0 : 1.0) : (double)acc;
+    }
+}
+
 // ----------------------------------------------------------------------------- reference CPU VBD
 // VertexBlockDescent::step (VertexBlockDescent.cpp:28-44), VBD_FEM::compute_inertia
 // (VBD_FEM.cpp:13-18), solve (:47-57), solve_vertex (:61-85), solve_element (:87-110),
@@ -1435,6 +1489,27 @@ int orc_vbd_residual(void* hv, float dt, double* out) {
     Handle* h = (Handle*)hv;
     if (h->kind == 1) residual_norms(*(VBD<double>*)h->ptr, (double)dt, out);
     else residual_norms(*(VBD<float>*)h->ptr, dt, out);
+    return 0;
+}
+int orc_vbd_forces(void* hv, float dt, double* out) {
+    Handle* h = (Handle*)hv;
+    if (!h || !out || h->kind > 1) return -1;
+    if (h->kind == 1) residual_vectors(*(VBD<double>*)h->ptr, (double)dt, out);
+    else residual_vectors(*(VBD<float>*)h->ptr, dt, out);
+    return 0;
+}
+int orc_element_data(void* hv, int kind, double* out) {
+    Handle* h = (Handle*)hv;
+    if (!h || !out || kind < 0 || kind > 4) return -1;
+    switch (h->kind) {
+        case 0: element_data(((VBD<float>*)h->ptr)->fem, ((VBD<float>*)h->ptr)->s, kind, out); break;
+        case 1: element_data(((VBD<double>*)h->ptr)->fem, ((VBD<double>*)h->ptr)->s, kind, out); break;
+        case 2: element_data(((XPBD<float>*)h->ptr)->fem, ((XPBD<float>*)h->ptr)->s, kind, out); break;
+        case 3: element_data(((XPBD<double>*)h->ptr)->fem, ((XPBD<double>*)h->ptr)->s, kind, out); break;
+        case 4: element_data(((Explicit<float>*)h->ptr)->fem, ((Explicit<float>*)h->ptr)->s, kind, out); break;
+        case 5: element_data(((Explicit<double>*)h->ptr)->fem, ((Explicit<double>*)h->ptr)->s, kind, out); break;
+        default: return -1;
+    }
     return 0;
 }
 void orc_vbd_destroy(void* hv) {

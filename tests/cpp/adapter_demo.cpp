@@ -1,7 +1,10 @@
 // Drives the reference-shaped C++ adapters (include/octopus_b200.hpp) the way
 // Cuda_VBD_FEM_Dynamic + Cuda_ParticleSystem_Dynamics do, on config 1 (8x2x2 P1 beam,
 // Stable Neo-Hookean E=1e5 nu=0.45, 20 iterations), and prints the final positions.
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "octopus_b200.hpp"
@@ -22,13 +25,20 @@ int main(int argc, char** argv) {
     auto* ps = new GPU_ParticleSystem(geometry, masses);
     auto* integrator = new GPU_VBD(ps, 20, 0.f);
     integrator->gravity[0] = 0.f; integrator->gravity[1] = 0.f; integrator->gravity[2] = -9.81f;
-    integrator->add_dynamics(new GPU_VBD_FEM(Tetra, T, geometry, Stable_NeoHooke, 1e5f, 0.45f, 0.f, Reduction_Symmetry, -1));
+    auto* fem = new GPU_VBD_FEM(Tetra, T, geometry, Stable_NeoHooke, 1e5f, 0.45f, 0.f, Reduction_Symmetry, -1);
+    integrator->add_dynamics(fem);
     integrator->add_constraint(new GPU_Fix_Constraint(geometry, new Plane(Vector3(0.01f, 0, 0), Vector3(-1, 0, 0))));
     const int sub_it = 1;
     for (int f = 0; f < frames; ++f)
         for (int i = 0; i < sub_it; ++i) integrator->step(ps, 0.01f / sub_it);
     ps->get_position(geometry);
     for (const Vector3& p : geometry) std::printf("%.9g %.9g %.9g\n", p.x, p.y, p.z);
+    // GPU_FEM queries: total volume, inverted elements, largest residual force
+    double volume = 0, inverted = 0, rmax = 0;
+    for (scalar v : fem->get_volume(ps)) volume += v;
+    for (scalar v : fem->get_inverted(ps)) inverted += v;
+    for (const Vector3& r : fem->get_forces(ps, 0.01f)) rmax = std::max(rmax, (double)std::fabs(r.z));
+    std::fprintf(stderr, "volume %.9g inverted %g rmax %.9g\n", volume, inverted, rmax);
     delete integrator;
     delete ps;
     return 0;

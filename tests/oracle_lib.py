@@ -66,6 +66,8 @@ def lib():
         L.orc_cpuvbd_run_many.argtypes = [C.POINTER(vp), C.c_int, C.c_float, C.c_int, C.c_int, C.c_int]
         L.orc_cpuvbd_run_many.restype = C.c_double
         L.orc_polar.argtypes = [dp, C.c_int, dp, dp]
+        L.orc_element_data.argtypes = [vp, C.c_int, dp]
+        L.orc_vbd_forces.argtypes = [vp, C.c_float, dp]
         L.orc_xpbd_pair.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, dp, dp, dp]
         _lib = L
     return _lib
@@ -227,6 +229,21 @@ class Solver:
         e = np.zeros(4)
         lib().orc_vbd_energy(self.h, _p(e, C.c_double))
         return e
+
+    def set(self, what, values):
+        """VBD state write (what: 0 p, 1 v, 2 last_p, 3 y)."""
+        a = np.ascontiguousarray(values, np.float64)
+        assert lib().orc_vbd_set(self.h, what, _p(a, C.c_double)) == 0
+
+    def element_data(self, kind):
+        out = np.zeros(self.scene.desc.n_elements)
+        assert lib().orc_element_data(self.h, kind, _p(out, C.c_double)) == 0
+        return out
+
+    def forces(self, dt):
+        out = np.zeros((self.scene.n, 3))
+        assert lib().orc_vbd_forces(self.h, dt, _p(out, C.c_double)) == 0
+        return out
 
     def residual(self, dt):
         r = np.zeros(2)

@@ -29,7 +29,10 @@ def test_adapter_compiles(built, tmp_path):
 @pytest.mark.gpu
 def test_adapter_matches_oracle(built, tmp_path):
     exe = _compile(tmp_path)
-    out = subprocess.check_output([exe, "5"], text=True)
+    run = subprocess.run([exe, "5"], text=True, capture_output=True, check=True)
+    out = run.stdout
+    diag = dict(zip(run.stderr.split()[::2], map(float, run.stderr.split()[1::2])))
+    assert abs(diag["volume"] - 1.0 * 0.25 * 0.25) < 1e-3 and diag["inverted"] == 0 and diag["rmax"] > 0
     p = np.array([[float(v) for v in ln.split()] for ln in out.strip().split("\n")])
     X, T = O.beam_mesh(O.TETRA, (8, 2, 2), (1.0, 0.25, 0.25))
     m = O.masses(O.TETRA, X, T, 1000.0, 1)
