@@ -22,8 +22,15 @@ Single-scene solver workloads of the P2 beam (64x16x16 hex grid x 6 tets = 98,30
   explicit_p2  one step = 100 symplectic-Euler sub-steps of dt = 1e-5 s, captured as a CUDA
                graph; metric vertex-steps/s
 
+Served stream ("served"): Poisson arrivals at each rate of --rates (requests/s, wall clock);
+each request is a seeded beam scene as in the batched workload with element count
+log-uniform in [1e3, 5e5] and step count uniform in [10, 200], admitted by the request loop
+(oct_server_*) under a 150 GB budget; one JSON line with, per rate, the aggregate
+vertex-iterations/s, p50/p99 device frame time, p50/p99 wall time per tick and per request,
+and the plain single-scene path on a sample of the same requests.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload batched|p2|cfg1|cube_p3|cube_q2|xpbd_p2|explicit_p2]
+                    [--workload batched|p2|cfg1|cube_p3|cube_q2|xpbd_p2|explicit_p2|served]
 """
 import argparse
 import concurrent.futures as cf
@@ -344,6 +351,137 @@ def bench_solver(args, world, rank, local, threads):
         torch.distributed.destroy_process_group()
 
 
+def served_request(rng):
+    """One request of the served stream: (element, cells, size, young, poisson, steps)."""
+    import octopusengine_b200 as ob
+    e = [ob.TETRA, ob.TETRA10, ob.HEXA][int(rng.integers(0, 3))]
+    target = float(np.exp(rng.uniform(np.log(1e3), np.log(5e5))))
+    cells = target / (1.0 if e == ob.HEXA else 6.0)
+    ny = max(2, int(round((cells / 4.0) ** (1.0 / 3.0))))
+    nx = max(4, int(round(cells / (ny * ny))))
+    young = float(np.exp(rng.uniform(np.log(1e4), np.log(1e7))))
+    nu = float(rng.uniform(0.30, 0.49))
+    return dict(element=e, cells=(nx, ny, ny), size=(nx / 16.0, ny / 16.0, ny / 16.0), young=young, poisson=nu,
+                density=1000.0, steps=int(rng.integers(10, 201)))
+
+
+def bench_served(args, threads):
+    """Continuous batching of a Poisson request stream through oct_server_* (one GPU)."""
+    import ctypes as C
+
+    import torch
+    import octopusengine_b200 as ob
+    from octopusengine_b200 import capi
+    torch.cuda.set_device(0)
+    iterations, substeps, frame_dt = 20, 4, FRAME_DT
+    rates = [float(x) for x in args.rates.split(",") if x]
+    ctx = ob.Context(0, 0)
+    results = []
+    for ri, rate in enumerate(rates):
+        rng = np.random.default_rng(args.seed + ri)
+        srv = ob.Server(ctx, frame_dt=frame_dt, substeps=substeps, iterations=iterations, max_scenes=1024,
+                        hbm_budget=150 * 10 ** 9, precision=ob.PREC_MIXED, setup_threads=max(1, threads - 2))
+        # the request stream is generated before the clock starts (arrival times and meshes), so
+        # the loop below only submits, ticks and polls
+        arrivals_at, reqs, t = [], [], rng.exponential(1.0 / rate)
+        while t < args.serve_seconds:
+            r = served_request(rng)
+            X, T = ob.beam_mesh(r["element"], r["cells"], r["size"])
+            fixed = ob.fixed_by_plane(X, (0.01, 0.0, 0.0), (-1.0, 0.0, 0.0))
+            reqs.append((r, X, T, fixed))
+            arrivals_at.append(t)
+            t += rng.exponential(1.0 / rate)
+        outstanding, latencies, tick_ms, nxt = {}, [], [], 0
+        finished_seen = 0
+        t_start = time.perf_counter()
+        with ClockSampler(0) as clocks:
+            while True:
+                now = time.perf_counter() - t_start
+                while nxt < len(reqs) and arrivals_at[nxt] <= now:
+                    r, X, T, fixed = reqs[nxt]
+                    rid = srv.submit(r["element"], X, T, r["steps"], density=1000.0, mass_distribution=ob.MASS_FEMSHAPE,
+                                     material=ob.STABLE_NEOHOOKE, young=r["young"], poisson=r["poisson"],
+                                     fixed_ids=fixed, gravity=(0.0, 0.0, -9.81))
+                    outstanding[rid] = t_start + arrivals_at[nxt]
+                    nxt += 1
+                if nxt >= len(reqs) and not outstanding:
+                    break
+                if now > args.serve_seconds * 4:   # drain limit
+                    break
+                t0 = time.perf_counter()
+                st0 = srv.stats()
+                srv.tick()
+                st1 = srv.stats()
+                if st1["frames"] > st0["frames"]:   # ticks that ran a frame
+                    tick_ms.append((time.perf_counter() - t0) * 1e3)
+                if st1["finished"] + st1["rejected"] > finished_seen:
+                    finished_seen = st1["finished"] + st1["rejected"]
+                    for rid in list(outstanding):
+                        if srv.poll(rid, fetch=False) is not None:
+                            latencies.append(time.perf_counter() - outstanding.pop(rid))
+                if not st1["active"]:
+                    time.sleep(0.001)   # idle: waiting for arrivals or set-up
+        arrivals = nxt
+        wall = time.perf_counter() - t_start
+        st = srv.stats()
+        results.append({
+            "rate_per_s": rate, "arrived": arrivals, "finished": int(st["finished"]), "rejected": int(st["rejected"]),
+            "frames": int(st["frames"]), "wall_s": wall,
+            "vertex_iter_per_s": st["vertex_iterations"] / wall,
+            "vertex_iter_per_busy_s": st["vertex_iterations"] / max(st["busy_ms"] * 1e-3, 1e-9),
+            "gpu_busy_frac": st["busy_ms"] * 1e-3 / wall,
+            "gap_ms_per_frame": st["gap_ms"] / max(st["frames"], 1),
+            "p50_step_ms": st["p50_step_ms"], "p99_step_ms": st["p99_step_ms"], "mean_step_ms": st["mean_step_ms"],
+            "p50_tick_wall_ms": float(np.percentile(tick_ms, 50)) if tick_ms else None,
+            "p99_tick_wall_ms": float(np.percentile(tick_ms, 99)) if tick_ms else None,
+            "p50_request_s": float(np.percentile(latencies, 50)) if latencies else None,
+            "p99_request_s": float(np.percentile(latencies, 99)) if latencies else None,
+            "clocks": clocks.summary()})
+        srv.close()
+    # plain single-scene path on a sample of the same request stream: each scene stepped alone
+    rng = np.random.default_rng(args.seed)
+    sample = [served_request(rng) for _ in range(12)]
+    scenes = []
+    for r in sample:
+        X, T = ob.beam_mesh(r["element"], r["cells"], r["size"])
+        fixed = ob.fixed_by_plane(X, (0.01, 0.0, 0.0), (-1.0, 0.0, 0.0))
+        scenes.append(ob.Scene(ctx, r["element"], X, T, density=1000.0, mass_distribution=ob.MASS_FEMSHAPE,
+                               material=ob.STABLE_NEOHOOKE, young=r["young"], poisson=r["poisson"], fixed_ids=fixed,
+                               gravity=(0.0, 0.0, -9.81), iterations=iterations, precision=ob.PREC_PLAIN))
+    stream_ptr = C.c_void_p()
+    capi.lib().oct_ctx_stream(ctx.handle, C.byref(stream_ptr))
+    stream = torch.cuda.ExternalStream(stream_ptr.value, device=0)
+    for sc in scenes:
+        sc.step(frame_dt, substeps, sync=False)
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    for _ in range(2):
+        for sc in scenes:
+            sc.step(frame_dt, substeps, sync=False)
+    p1.record(stream)
+    torch.cuda.synchronize()
+    vit = 2 * sum(sc.n_nodes - sc.n_fixed for sc in scenes) * iterations * substeps
+    plain = vit / (p0.elapsed_time(p1) * 1e-3)
+    for sc in scenes:
+        sc.close()
+    top = max(results, key=lambda x: x["vertex_iter_per_s"])
+    print(json.dumps({
+        "metric": "vertex_iterations_per_s", "value": top["vertex_iter_per_s"], "unit": "vertex-iter/s", "n_gpus": 1,
+        "steps": int(top["frames"]), "warmup": 0, "ms_per_step": top["mean_step_ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "served", "rates_per_s": rates, "serve_seconds": args.serve_seconds,
+                   "iterations": iterations, "substeps": substeps, "frame_dt": frame_dt, "budget_bytes": 150 * 10 ** 9,
+                   "seed": args.seed, "precision": "mixed"},
+        "p50_step_ms": top["p50_step_ms"], "p99_step_ms": top["p99_step_ms"],
+        "served": results,
+        "plain_dropin": {"value": plain, "unit": "vertex-iter/s",
+                         "path": "12 requests of the stream, each scene stepped alone (FP32, per-colour launches)"},
+        "batched_over_plain": top["vertex_iter_per_busy_s"] / plain,
+        "gpu_launches": None}))
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -351,12 +489,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched",
-                    choices=["batched", "p2", "cfg1", "cube_p3", "cube_q2", "xpbd_p2", "explicit_p2"])
+                    choices=["batched", "p2", "cfg1", "cube_p3", "cube_q2", "xpbd_p2", "explicit_p2", "served"])
+    ap.add_argument("--rates", default="4,8,16", help="served: Poisson arrival rates (requests/s)")
+    ap.add_argument("--serve-seconds", type=float, default=20.0, help="served: arrival window per rate")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tpv", type=int, default=0, help="lanes per vertex (0 = measured default, -1 = packed pair-per-lane mapping)")
     ap.add_argument("--tpv-elem", default="", help="per-element lanes per vertex, e.g. 3:4,7:-1")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the measured default mapping")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -366,6 +507,14 @@ def main():
     threads = os.cpu_count() or 1
     if args.workload in SOLVER_WORKLOADS:
         bench_solver(args, world, rank, local, threads)
+        return
+    if args.workload == "served":
+        if args.impl == "reference" or rank != 0:
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no request loop; "
+                                  "its CPU VBD path is timed by the batched workload"}))
+            return
+        bench_served(args, threads)
         return
     specs, iterations, substeps, frame_dt = workload_specs(args.workload, args.seed)
 
@@ -409,6 +558,13 @@ def main():
         scenes = list(ex.map(lambda a: build_scene(ctx, a[1], iterations, ob.PREC_MIXED, args.seed + a[0],
                                                    per_elem.get(a[1]["element"], args.tpv)), enumerate(specs)))
     setup_s = time.time() - t0
+    # lane mapping per element type: the autotuner times every candidate on these scenes
+    # (state untouched) unless a mapping was forced on the command line
+    mapping, tune_s = None, None
+    if not args.no_autotune and args.tpv == 0 and not args.tpv_elem:
+        t0 = time.time()
+        mapping = ob.autotune_mapping(ctx, scenes, frame_dt / substeps, sweeps=3)
+        tune_s = time.time() - t0
     batch = ob.Batch(ctx, scenes)
     free_nodes = sum(s.n_nodes - s.n_fixed for s in scenes)
     vit_per_step = free_nodes * iterations * substeps
@@ -566,6 +722,9 @@ def main():
                        "iterations": iterations, "substeps": substeps, "frame_dt": frame_dt,
                        "precision": "mixed (FP32 bulk, compensated sums, FP64 ill-conditioned solves)",
                        "seed": args.seed, "l2": "state larger than L2 (126 MB); no flush",
+                       "mapping": ({str(k): v for k, v in mapping.items()} if mapping is not None else
+                                   "fixed (--tpv / --tpv-elem / --no-autotune)"),
+                       "autotune_s": tune_s,
                        "parallelism": "replicas" if world > 1 else "single GPU"},
             "p50_step_ms": float(np.percentile(step_ms, 50)), "p99_step_ms": float(np.percentile(step_ms, 99)),
             "plain_dropin": plain,

@@ -180,8 +180,23 @@ oct_status oct_scene_vertex_residuals(oct_scene* s, float dt, float* out_n3);
 /* Batch: many VBD scenes stepped together, one launch per (element type, colour) across all
  * scenes, driven by a per-scene work table, the sub-step captured as a CUDA graph.  All
  * scenes must be VBD scenes of this context with equal iteration counts. */
+/* Lane mapping of a VBD or explicit scene's vertex kernel (same values as
+ * oct_scene_desc.threads_per_vertex: -1 packed pairs, 0 measured default, 1..32 lanes per
+ * vertex).  OCT_ENOTSUP for the packed mapping when a vertex has more than 32 owners. */
+oct_status oct_scene_set_mapping(oct_scene* s, int threads_per_vertex);
+/* Mapping autotuner (new): for each element type among the scenes, times one colour sweep of
+ * all its scenes under every candidate mapping (packed pairs, 1, 2, 4, 8, 16, 32 lanes per
+ * vertex) and sets the fastest on those scenes.  The timed sweeps write only the Jacobi
+ * scratch buffer, so positions and velocities are unchanged.  chosen (may be NULL): per
+ * element id the mapping picked (-1 packed), 0 for element types absent.  Run it before
+ * oct_batch_create; it leaves no batch behind. */
+oct_status oct_autotune_mapping(oct_ctx* ctx, oct_scene* const* scenes, int n, float dt, int sweeps, int32_t chosen[10]);
 oct_status oct_batch_create(oct_ctx* ctx, oct_scene* const* scenes, int n, oct_batch** out);
 oct_status oct_batch_step(oct_batch* b, float frame_dt, int substeps);
+/* Captures the sub-step graph for (frame_dt, substeps) without launching it, so that a later
+ * oct_batch_step starts at once (the serving loop prepares the next batch this way while the
+ * current frame runs). */
+oct_status oct_batch_prepare(oct_batch* b, float frame_dt, int substeps);
 oct_status oct_batch_destroy(oct_batch* b);
 /* End-to-end helpers: upload all scenes' positions+velocities from one host array (scene
  * order, n_i*6 floats each: p then v) and read them back. */
@@ -233,6 +248,7 @@ typedef struct oct_server_stats {
     double vertex_iterations;                         /* total free-vertex updates done */
     double busy_ms;                                   /* summed device time of the frames */
     size_t bytes_in_use;
+    double gap_ms;      /* device idle time between consecutive frames of a busy period */
 } oct_server_stats;
 
 oct_status oct_server_create(oct_ctx* ctx, const oct_server_config* cfg, oct_server** out);

@@ -25,7 +25,7 @@ from .capi import (COLOR_DSAT, COLOR_GREEDY, COROTATED, ELEMENT_NODES, FIXED_COR
                    VBD_BETTER_COLORATION, VBD_REDUCTION_SYMMETRY, XPBD_OPTIGROUP, XPBD_OPTISHARED, XPBD_QUADRATURE,
                    XPBD_XPBD, OctError, beam_mesh, color, fixed_by_plane, lumped_masses, shape_table)
 
-__all__ = ["Context", "Scene", "Batch", "Server", "make_desc", "OctError", "beam_mesh", "color", "lumped_masses", "shape_table",
+__all__ = ["Context", "Scene", "Batch", "Server", "make_desc", "autotune_mapping", "OctError", "beam_mesh", "color", "lumped_masses", "shape_table",
            "fixed_by_plane", "library_path"]
 
 
@@ -126,6 +126,11 @@ class Scene:
     def handle(self):
         return self._h
 
+    def set_mapping(self, threads_per_vertex):
+        """Lane mapping of the vertex kernel (-1 packed, 0 default, 1..32 lanes per vertex)."""
+        capi.check(capi.lib().oct_scene_set_mapping(self._h, int(threads_per_vertex)), "oct_scene_set_mapping",
+                   self.ctx.handle)
+
     def set_capture(self, on=True):
         """Replay each frame's sub-steps from a captured CUDA graph (oct_scene_set_capture)."""
         capi.check(capi.lib().oct_scene_set_capture(self._h, int(on)), "oct_scene_set_capture", self.ctx.handle)
@@ -211,6 +216,17 @@ class Scene:
             self._h = C.c_void_p()
 
 
+def autotune_mapping(ctx, scenes, dt, sweeps=3):
+    """Times every lane mapping per element type over the scenes and keeps the fastest
+    (oct_autotune_mapping); returns {element: mapping} (-1 = packed pairs)."""
+    arr = (C.c_void_p * len(scenes))(*[s.handle.value for s in scenes])
+    chosen = (C.c_int32 * 10)()
+    capi.check(capi.lib().oct_autotune_mapping(ctx.handle, arr, len(scenes), dt, sweeps, chosen),
+               "oct_autotune_mapping", ctx.handle)
+    present = {s.element for s in scenes}
+    return {e: int(chosen[e]) for e in present}
+
+
 class Batch:
     """Many VBD scenes stepped together (one launch per element type and colour, CUDA graph)."""
 
@@ -266,13 +282,16 @@ class Server:
         capi.check(capi.lib().oct_server_tick(self._h, C.byref(n)), "oct_server_tick", self.ctx.handle)
         return n.value
 
-    def poll(self, rid):
+    def poll(self, rid, fetch=True):
+        """None while the request runs; then its final positions (or True with fetch=False)."""
         done = C.c_int32()
-        out = np.zeros((self.n_nodes[rid], 3), np.float32)
-        st = capi.lib().oct_server_poll(self._h, rid, C.byref(done), capi.ptr(out, C.c_float))
+        out = np.zeros((self.n_nodes[rid], 3), np.float32) if fetch else None
+        st = capi.lib().oct_server_poll(self._h, rid, C.byref(done), capi.ptr(out, C.c_float) if fetch else None)
         if st != capi.OK:
             raise OctError(st, "oct_server_poll")
-        return (out if done.value else None)
+        if not done.value:
+            return None
+        return out if fetch else True
 
     def stats(self):
         s = capi.ServerStats()

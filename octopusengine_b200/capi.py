@@ -39,7 +39,8 @@ EXPORTS = [
     "oct_batch_group_info", "oct_batch_time_group", "oct_scene_set_precision", "oct_scene_footprint",
     "oct_server_create", "oct_server_submit", "oct_server_tick", "oct_server_poll", "oct_server_get_stats",
     "oct_server_destroy", "oct_elastic_energy_noalloc", "oct_scene_set_fixation_group",
-    "oct_scene_element_data", "oct_scene_vertex_residuals",
+    "oct_scene_element_data", "oct_scene_vertex_residuals", "oct_scene_set_mapping", "oct_autotune_mapping",
+    "oct_batch_prepare",
 ]
 
 
@@ -53,7 +54,8 @@ class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("finished", C.c_int64),
                 ("rejected", C.c_int64), ("queued", C.c_int64), ("active", C.c_int64), ("frames", C.c_int64),
                 ("p50_step_ms", C.c_double), ("p99_step_ms", C.c_double), ("mean_step_ms", C.c_double),
-                ("vertex_iterations", C.c_double), ("busy_ms", C.c_double), ("bytes_in_use", C.c_size_t)]
+                ("vertex_iterations", C.c_double), ("busy_ms", C.c_double), ("bytes_in_use", C.c_size_t),
+                ("gap_ms", C.c_double)]
 
 
 class SceneDesc(C.Structure):
@@ -101,6 +103,9 @@ def lib():
             "oct_scene_sync": ([vp], C.c_int),
             "oct_scene_set_capture": ([vp, C.c_int], C.c_int),
             "oct_scene_element_data": ([vp, C.c_int, C.POINTER(C.c_float)], C.c_int),
+            "oct_scene_set_mapping": ([vp, C.c_int], C.c_int),
+            "oct_batch_prepare": ([vp, C.c_float, C.c_int], C.c_int),
+            "oct_autotune_mapping": ([vp, C.POINTER(vp), C.c_int, C.c_float, C.c_int, C.POINTER(C.c_int32)], C.c_int),
             "oct_scene_vertex_residuals": ([vp, C.c_float, C.POINTER(C.c_float)], C.c_int),
             "oct_scene_get_positions": ([vp, fp], C.c_int),
             "oct_scene_get_velocities": ([vp, fp], C.c_int),

@@ -88,7 +88,7 @@ struct oct_scene {
     DevMem mem;
     int solver = 0, element = 0, material = 0, ne = 0, nq = 0;
     int n_nodes = 0, n_elements = 0, n_fixed = 0, n_colors = 0;
-    int iterations = 1, order_mode = 0, tpv = 8, precision = 0;
+    int iterations = 1, order_mode = 0, tpv = 8, precision = 0, max_valence = 0;
     float rho = 0.f, global_damping = 0.f;
     bool in_place = true, box = false, has_v0 = false;
     bool xpbd_raw = true, xpbd_project = true;   // XPBD update form; false: no projection (OptiGroup)
@@ -232,6 +232,17 @@ oct_status check_error_word(oct_ctx* c) {
     if (e & 2) { int z = 0; cudaMemcpy(c->d_error, &z, sizeof(int), cudaMemcpyHostToDevice); return fail(c, OCT_ENUMERIC, "non-finite value in the scene state"); }
     if (e & 1) { int z = 0; cudaMemcpy(c->d_error, &z, sizeof(int), cudaMemcpyHostToDevice); return fail(c, OCT_ETIMEDOUT, "a bounded device wait timed out"); }
     return OCT_OK;
+}
+
+// Vertex work items of every colour for the scene's lane mapping (tpv), uploaded to the device.
+oct_status build_vertex_work(oct_scene* s) {
+    std::vector<VWork> vw;
+    s->vwork_off.assign(1, 0);
+    for (int k = 0; k + 1 < (int)s->color_off.size(); ++k) {
+        append_vwork(vw, 0, s->color_off[k], s->color_off[k + 1], s->tpv, s->own_off);
+        s->vwork_off.push_back((int)vw.size());
+    }
+    return upload(s->ctx, s->mem, s->d_vwork, vw);
 }
 
 oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
@@ -451,6 +462,7 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     // warps; vertices with more than 32 owners fall back to a lane group per vertex
     if (d->threads_per_vertex == 0) s->tpv = measured_tpv(d->element);
     if (s->tpv == 0 && max_valence > 32) s->tpv = max_valence > 64 ? 32 : default_tpv(d->element);
+    s->max_valence = max_valence;
     s->own_off = own_off;
 
     // device state
@@ -516,19 +528,13 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     if ((st = s->mem.alloc(s->d_red, 4))) return st;
 
     // work tables
-    std::vector<VWork> vw;
-    s->vwork_off.assign(1, 0);
-    for (int k = 0; k + 1 < (int)s->color_off.size(); ++k) {
-        append_vwork(vw, 0, s->color_off[k], s->color_off[k + 1], s->tpv, s->own_off);
-        s->vwork_off.push_back((int)vw.size());
-    }
+    if ((st = build_vertex_work(s))) return st;
     std::vector<NWork> nw, fw;
     append_nwork(nw, 0, N);
     append_nwork(fw, 0, s->n_fixed);
     s->n_nwork = (int)nw.size();
     s->n_fwork = (int)fw.size();
-    if ((st = upload(c, s->mem, s->d_vwork, vw)) || (st = upload(c, s->mem, s->d_nwork, nw)) || (st = upload(c, s->mem, s->d_fwork, fw)))
-        return st;
+    if ((st = upload(c, s->mem, s->d_nwork, nw)) || (st = upload(c, s->mem, s->d_fwork, fw))) return st;
     return OCT_OK;
 }
 
@@ -1078,19 +1084,26 @@ uint64_t batch_launches_per_substep(const oct_batch* b) {
 }
 }  // namespace
 
-oct_status oct_batch_step(oct_batch* b, float frame_dt, int substeps) {
+oct_status oct_batch_prepare(oct_batch* b, float frame_dt, int substeps) {
     if (!b || substeps <= 0 || !(frame_dt > 0.f)) return OCT_EINVAL;
     oct_ctx* c = b->ctx;
     const float sub = frame_dt / (float)substeps;
-    if (!b->exec || b->graph_dt != sub) {
-        if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
-        if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
-        OCT_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        batch_substep(b, sub);
-        OCT_CUDA(c, cudaStreamEndCapture(c->stream, &b->graph));
-        OCT_CUDA(c, cudaGraphInstantiate(&b->exec, b->graph, 0));
-        b->graph_dt = sub;
-    }
+    if (b->exec && b->graph_dt == sub) return OCT_OK;
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    OCT_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    batch_substep(b, sub);
+    OCT_CUDA(c, cudaStreamEndCapture(c->stream, &b->graph));
+    OCT_CUDA(c, cudaGraphInstantiate(&b->exec, b->graph, 0));
+    b->graph_dt = sub;
+    return OCT_OK;
+}
+
+oct_status oct_batch_step(oct_batch* b, float frame_dt, int substeps) {
+    if (!b || substeps <= 0 || !(frame_dt > 0.f)) return OCT_EINVAL;
+    oct_ctx* c = b->ctx;
+    oct_status st = oct_batch_prepare(b, frame_dt, substeps);
+    if (st) return st;
     cudaEventRecord(c->ev0, c->stream);
     for (int k = 0; k < substeps; ++k) {
         OCT_CUDA(c, cudaGraphLaunch(b->exec, c->stream));
@@ -1161,6 +1174,88 @@ oct_status oct_batch_time_group(oct_batch* b, int g, int sweeps, float dt, float
     OCT_CUDA(c, cudaEventSynchronize(c->ev1));
     OCT_CUDA(c, cudaGetLastError());
     cudaEventElapsedTime(ms, c->ev0, c->ev1);
+    return OCT_OK;
+}
+
+oct_status oct_scene_set_mapping(oct_scene* s, int tpv) {
+    if (!s) return OCT_EINVAL;
+    if (s->solver == OCT_SOLVER_XPBD) return OCT_OK;   // element-centric: no vertex mapping
+    int t = tpv < 0 ? 0 : (tpv == 0 ? measured_tpv(s->element) : tpv);
+    if (tpv < -1 || (t != 0 && t != 1 && t != 2 && t != 4 && t != 8 && t != 16 && t != 32))
+        return fail(s->ctx, OCT_EINVAL, "threads_per_vertex must be -1 (packed), 0 (default) or a power of two <= 32");
+    if (t == 0 && s->max_valence > 32) {
+        if (tpv < 0) return fail(s->ctx, OCT_ENOTSUP, "packed mapping needs at most 32 owners per vertex");
+        t = s->max_valence > 64 ? 32 : default_tpv(s->element);
+    }
+    OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    s->tpv = t;
+    drop_frame_graph(s);
+    return build_vertex_work(s);
+}
+
+// Times one colour sweep of every group of a batch with the solve results written to the
+// Jacobi buffer (u_new) and not committed, so the scenes' state is left as it was.
+static oct_status time_batch_sweeps(oct_batch* b, int sweeps, float dt, float* ms) {
+    oct_ctx* c = b->ctx;
+    StepParams P = base_params(c, dt);
+    P.in_place = 0;
+    OCT_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+    for (int r = 0; r < sweeps; ++r)
+        for (const auto& G : b->groups)
+            for (size_t k = 0; k + 1 < G.off.size(); ++k) {
+                const int n = G.off[k + 1] - G.off[k];
+                launch_vertex(G.element, G.material, b->d_scenes, b->d_vwork + G.base + G.off[k], n, G.tpv, 0, P, nullptr,
+                              c->stream);
+            }
+    OCT_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+    OCT_CUDA(c, cudaEventSynchronize(c->ev1));
+    OCT_CUDA(c, cudaGetLastError());
+    cudaEventElapsedTime(ms, c->ev0, c->ev1);
+    return OCT_OK;
+}
+
+oct_status oct_autotune_mapping(oct_ctx* c, oct_scene* const* scenes, int n, float dt, int sweeps, int32_t chosen[10]) {
+    if (!c || !scenes || n <= 0 || !(dt > 0.f) || sweeps <= 0) return OCT_EINVAL;
+    if (chosen) std::fill(chosen, chosen + 10, 0);
+    std::map<int, std::vector<oct_scene*>> by_element;
+    for (int i = 0; i < n; ++i) {
+        if (!scenes[i] || scenes[i]->ctx != c) return fail(c, OCT_EINVAL, "scene from another context");
+        if (scenes[i]->solver == OCT_SOLVER_XPBD) continue;
+        by_element[scenes[i]->element].push_back(scenes[i]);
+    }
+    for (auto& [element, list] : by_element) {
+        int max_val = 0;
+        for (auto* s : list) max_val = std::max(max_val, s->max_valence);
+        std::vector<int> cands = {1, 2, 4, 8, 16, 32};
+        if (max_val <= 32) cands.insert(cands.begin(), -1);
+        const std::vector<int> old = [&] { std::vector<int> v; for (auto* s : list) v.push_back(s->tpv); return v; }();
+        float best_ms = 1e30f;
+        int best = 0;
+        for (int cand : cands) {
+            for (auto* s : list) s->tpv = cand < 0 ? 0 : cand;   // host field only: the batch builds its own tables
+            oct_batch* b = nullptr;
+            oct_status st = oct_batch_create(c, list.data(), (int)list.size(), &b);
+            if (st) {
+                for (size_t i = 0; i < list.size(); ++i) list[i]->tpv = old[i];
+                return st;
+            }
+            float ms = 0.f;
+            st = time_batch_sweeps(b, 1, dt, &ms);   // warm-up
+            if (!st) st = time_batch_sweeps(b, sweeps, dt, &ms);
+            oct_batch_destroy(b);
+            if (st) {
+                for (size_t i = 0; i < list.size(); ++i) list[i]->tpv = old[i];
+                return st;
+            }
+            if (ms < best_ms) { best_ms = ms; best = cand; }
+        }
+        for (size_t i = 0; i < list.size(); ++i) list[i]->tpv = old[i];
+        for (auto* s : list) {
+            oct_status st = oct_scene_set_mapping(s, best);
+            if (st) return st;
+        }
+        if (chosen && element >= 0 && element < 10) chosen[element] = best;
+    }
     return OCT_OK;
 }
 

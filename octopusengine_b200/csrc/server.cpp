@@ -7,6 +7,10 @@
 // larger than the whole budget is rejected at submit.  Set-up of admitted scenes (mesh
 // graphs, colouring, FP64 precompute, upload) runs on host worker threads while the GPU
 // advances the current batch; ready scenes join the batch at the next frame boundary.
+// Membership changes are known while a frame runs (the requests on their last step, the
+// scenes whose set-up finished), so the next frame's batch is built and its graph captured
+// during the current frame; the GPU then goes from one frame to the next without waiting
+// on the host.
 #include <algorithm>
 #include <chrono>
 #include <cstring>
@@ -50,14 +54,16 @@ struct oct_server {
     size_t budget = 0, reserved = 0;
     int64_t next_id = 1;
     std::deque<Request*> queue;
-    std::vector<Request*> staging, active;
+    std::vector<Request*> staging, active, joining;   // joining: set up, enter at the next frame
     std::map<int64_t, std::unique_ptr<Request>> all;
     oct_batch* batch = nullptr;
     bool dirty = true;
     std::vector<double> frame_ms;
     double vertex_iterations = 0, busy_ms = 0;
     int64_t submitted = 0, admitted = 0, finished = 0, rejected = 0;
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, prev_end = nullptr;
+    bool have_prev = false;
+    double gap_ms = 0;   // device idle time between consecutive frames
     cudaStream_t stream = nullptr;
 };
 
@@ -75,7 +81,8 @@ oct_status oct_server_create(oct_ctx* ctx, const oct_server_config* cfg, oct_ser
     void* st = nullptr;
     oct_ctx_stream(ctx, &st);
     s->stream = (cudaStream_t)st;
-    if (cudaEventCreate(&s->e0) != cudaSuccess || cudaEventCreate(&s->e1) != cudaSuccess) { delete s; return OCT_ECUDA; }
+    if (cudaEventCreate(&s->e0) != cudaSuccess || cudaEventCreate(&s->e1) != cudaSuccess ||
+        cudaEventCreate(&s->prev_end) != cudaSuccess) { delete s; return OCT_ECUDA; }
     *out = s;
     return OCT_OK;
 }
@@ -136,8 +143,7 @@ void collect_ready(oct_server* s, bool wait_all) {
             int32_t nn = 0, nf = 0;
             oct_scene_info(r->scene, &nn, nullptr, nullptr, &nf);
             r->free_nodes = nn - nf;
-            s->active.push_back(r);
-            s->dirty = true;
+            s->joining.push_back(r);
         } else {
             r->done = true;
             s->reserved -= r->bytes;
@@ -145,6 +151,16 @@ void collect_ready(oct_server* s, bool wait_all) {
         }
         it = s->staging.erase(it);
     }
+}
+
+oct_status build_batch(oct_server* s, const std::vector<Request*>& members, oct_batch** out) {
+    *out = nullptr;
+    if (members.empty()) return OCT_OK;
+    std::vector<oct_scene*> sc;
+    for (auto* r : members) sc.push_back(r->scene);
+    oct_status st = oct_batch_create(s->ctx, sc.data(), (int)sc.size(), out);
+    if (st) return st;
+    return oct_batch_prepare(*out, s->cfg.frame_dt, s->cfg.substeps);
 }
 
 void admit(oct_server* s) {
@@ -166,48 +182,70 @@ void admit(oct_server* s) {
 
 oct_status oct_server_tick(oct_server* s, int32_t* n_active) {
     if (!s) return OCT_EINVAL;
-    collect_ready(s, false);
     admit(s);
-    if (s->active.empty() && !s->staging.empty()) collect_ready(s, true);   // nothing to overlap with
+    // scenes join while a frame runs; only an idle server takes them here (waiting for a set-up
+    // when there is nothing else to do)
+    if (s->active.empty()) {
+        collect_ready(s, false);
+        if (s->joining.empty() && !s->staging.empty()) collect_ready(s, true);
+    }
+    if (!s->joining.empty() || s->dirty) {   // membership changed outside a frame
+        s->active.insert(s->active.end(), s->joining.begin(), s->joining.end());
+        s->joining.clear();
+        if (s->batch) { oct_batch_destroy(s->batch); s->batch = nullptr; }
+        oct_status st = build_batch(s, s->active, &s->batch);
+        if (st) return st;
+        s->dirty = false;
+    }
     if (!s->active.empty()) {
-        if (s->dirty) {
-            if (s->batch) { oct_batch_destroy(s->batch); s->batch = nullptr; }
-            std::vector<oct_scene*> sc;
-            for (auto* r : s->active) sc.push_back(r->scene);
-            oct_status st = oct_batch_create(s->ctx, sc.data(), (int)sc.size(), &s->batch);
-            if (st) return st;
-            s->dirty = false;
-        }
         cudaEventRecord(s->e0, s->stream);
         oct_status st = oct_batch_step(s->batch, s->cfg.frame_dt, s->cfg.substeps);
         if (st) return st;
         cudaEventRecord(s->e1, s->stream);
-        admit(s);                           // set-up of queued requests overlaps the frame
+        // while the frame runs: start queued set-ups, collect finished ones and build the next
+        // frame's batch (members without the requests on their last step, plus the joiners)
+        admit(s);
+        collect_ready(s, false);
+        std::vector<Request*> next;
+        bool leaving = false;
+        for (auto* r : s->active) {
+            if (r->steps_done + 1 >= r->steps_total) leaving = true;
+            else next.push_back(r);
+        }
+        next.insert(next.end(), s->joining.begin(), s->joining.end());
+        oct_batch* next_batch = nullptr;
+        const bool changed = leaving || !s->joining.empty();
+        if (changed && (st = build_batch(s, next, &next_batch))) return st;
         if (cudaEventSynchronize(s->e1) != cudaSuccess) return OCT_ECUDA;
-        float ms = 0.f;
+        float ms = 0.f, gap = 0.f;
         cudaEventElapsedTime(&ms, s->e0, s->e1);
+        if (s->have_prev && cudaEventElapsedTime(&gap, s->prev_end, s->e0) == cudaSuccess) s->gap_ms += gap;
+        cudaEventRecord(s->prev_end, s->stream);   // the frame's end, for the next gap
+        s->have_prev = true;
         s->frame_ms.push_back(ms);
         s->busy_ms += ms;
-        for (auto it = s->active.begin(); it != s->active.end();) {
-            Request* r = *it;
+        if (changed) {   // the finished frame's batch is no longer needed
+            oct_batch_destroy(s->batch);
+            s->batch = next_batch;
+        }
+        for (auto* r : s->active) {
             s->vertex_iterations += (double)r->free_nodes * s->cfg.iterations * s->cfg.substeps;
             if (++r->steps_done >= r->steps_total) {
                 r->result.resize(3 * (size_t)r->desc.n_nodes);
                 r->status = oct_scene_get_positions(r->scene, r->result.data());
-                if (s->batch) { oct_batch_destroy(s->batch); s->batch = nullptr; }
                 oct_scene_destroy(r->scene);
                 r->scene = nullptr;
                 r->done = true;
                 s->reserved -= r->bytes;
                 s->finished++;
-                s->dirty = true;
-                it = s->active.erase(it);
-            } else {
-                ++it;
             }
         }
+        if (changed) {
+            s->active = next;
+            s->joining.clear();
+        }
     }
-    collect_ready(s, false);
+    if (s->active.empty()) s->have_prev = false;   // idle: the next gap is not a host delay
     if (n_active) *n_active = (int32_t)s->active.size();
     return OCT_OK;
 }
@@ -235,6 +273,7 @@ oct_status oct_server_get_stats(oct_server* s, oct_server_stats* o) {
     o->vertex_iterations = s->vertex_iterations;
     o->busy_ms = s->busy_ms;
     o->bytes_in_use = s->reserved;
+    o->gap_ms = s->gap_ms;
     if (!s->frame_ms.empty()) {
         std::vector<double> v(s->frame_ms);
         std::sort(v.begin(), v.end());
@@ -258,8 +297,10 @@ oct_status oct_server_destroy(oct_server* s) {
     collect_ready(s, true);
     if (s->batch) oct_batch_destroy(s->batch);
     for (auto* r : s->active) if (r->scene) oct_scene_destroy(r->scene);
+    for (auto* r : s->joining) if (r->scene) oct_scene_destroy(r->scene);
     cudaEventDestroy(s->e0);
     cudaEventDestroy(s->e1);
+    cudaEventDestroy(s->prev_end);
     delete s;
     return OCT_OK;
 }

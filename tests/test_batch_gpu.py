@@ -73,3 +73,47 @@ def test_batch_rejects_mismatched_iterations(ctx):
     b = ob.Scene(ctx, O.TETRA, X, T, iterations=4)
     with pytest.raises(ob.OctError):
         ob.Batch(ctx, [a, b])
+
+
+def test_autotune_keeps_state_and_picks_a_valid_mapping(ctx):
+    """oct_autotune_mapping times every mapping without touching positions or velocities; the
+    scenes then step exactly as scenes created with the chosen mapping."""
+    import octopusengine_b200 as ob
+    rng = np.random.default_rng(5)
+    specs = _mix(ctx, rng, 9)
+    tuned = [ob.Scene(ctx, e, X, T, **kw) for e, X, T, kw in specs]
+    for s in tuned:
+        s.step(1 / 60, 2)
+    before = [(s.get_position(), s.get_velocity()) for s in tuned]
+    chosen = ob.autotune_mapping(ctx, tuned, 1 / 240, sweeps=2)
+    assert set(chosen) == {O.TETRA, O.TETRA10, O.HEXA}
+    assert all(v in (-1, 1, 2, 4, 8, 16, 32) for v in chosen.values())
+    for s, (p, v) in zip(tuned, before):
+        np.testing.assert_array_equal(s.get_position(), p)
+        np.testing.assert_array_equal(s.get_velocity(), v)
+    ref = []
+    for (e, X, T, kw) in specs:   # same history: default mapping for the first frame, then the chosen one
+        r = ob.Scene(ctx, e, X, T, **kw)
+        r.step(1 / 60, 2)
+        r.set_mapping(chosen[e])
+        ref.append(r)
+    batch = ob.Batch(ctx, tuned)
+    rbatch = ob.Batch(ctx, ref)
+    for _ in range(2):
+        batch.step(1 / 60, 2)
+        rbatch.step(1 / 60, 2)
+    for a, b in zip(tuned, ref):
+        np.testing.assert_array_equal(a.get_position(), b.get_position())
+
+
+@pytest.mark.parametrize("mapping", [-1, 1, 2, 8])
+def test_set_mapping_mid_run_matches_oracle(ctx, mapping):
+    s, o32, o64, mesh = pair(ctx, O.TETRA10, cells=(4, 2, 2), iterations=6)
+    s.step(1 / 60, 2)
+    o64.step(1 / 60, 2)
+    s.set_mapping(mapping)
+    s.set_capture(True)
+    for _ in range(2):
+        s.step(1 / 60, 2)
+        o64.step(1 / 60, 2)
+    assert rel_err(s.get_position(), o64.get(0)) < 1e-5
