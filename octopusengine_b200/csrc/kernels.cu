@@ -511,8 +511,12 @@ template <int E> constexpr int packed_smem_bytes() { return (kBlock / 32) * 2 * 
 
 // ------------------------------------------------------------------------ colour kernel
 // mode 0: VBD solve; mode 1: VBD residual (r into u_new, |r| reductions); mode 2: explicit force.
+// Resident blocks per SM the lane-group kernel is compiled for: P2 and Q1 are held to 128
+// registers (4 blocks, 16 warps per SM; ptxas spills a few bytes), P1 to 80.
+template <int E> struct LaneMinBlocks { static constexpr int value = E == 3 ? 6 : (E == 6 || E == 7 ? 4 : 1); };
+
 template <int E, int MAT>
-__global__ void __launch_bounds__(kBlock, E == 3 ? 6 : 1) k_vertex(const SceneDev* __restrict__ scenes, const VWork* __restrict__ work,
+__global__ void __launch_bounds__(kBlock, LaneMinBlocks<E>::value) k_vertex(const SceneDev* __restrict__ scenes, const VWork* __restrict__ work,
                                                    int n_work, int tpv, int mode, StepParams P, double* red) {
     constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ;
     __shared__ __align__(128) float s_dN[((NQ * NE * 3 + 3) / 4) * 4];
