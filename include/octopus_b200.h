@@ -142,6 +142,15 @@ oct_status oct_scene_info(oct_scene* s, int32_t* n_nodes, int32_t* n_elements, i
 oct_status oct_scene_get_coloring(oct_scene* s, int32_t* colors, int32_t* vertex_order);
 /* Lumped masses used by the scene (compute_fem_mass). */
 oct_status oct_scene_get_masses(oct_scene* s, float* out_n);
+/* Element type, rest positions (n_nodes*3) and topology (n_elements*nodes_per_element) of a
+ * scene, as given at creation (GPU_FEM's mesh; the VTK recorder writes them). */
+oct_status oct_scene_element_type(oct_scene* s, int32_t* element);
+oct_status oct_scene_get_rest_positions(oct_scene* s, float* out_n3);
+oct_status oct_scene_get_topology(oct_scene* s, int32_t* out);
+/* Run metadata in the JSON of MeshRecorder and FEM_Dynamic_Recorder::add_data_json
+ * (octopus/src/Script/Record/Recorder.cpp:12-36): {"mesh" : {...}, "fem" : {...}}.  With out
+ * NULL only *length is set; otherwise capacity must hold length + 1 bytes. */
+oct_status oct_scene_metadata_json(oct_scene* s, char* out, size_t capacity, size_t* length);
 /* Move the fixed nodes rigidly: p = offset + com + R (init_p - com), R column-major 3x3
  * (GPU_Fix_Constraint axis, octopus/src/GPU/GPU_Constraint.cu:108-112).  _group addresses
  * one of the four rigid groups (oct_scene_set_fixation is group 0); batches holding the
@@ -262,6 +271,67 @@ oct_status oct_server_tick(oct_server* srv, int32_t* n_active);
 oct_status oct_server_poll(oct_server* srv, int64_t request_id, int32_t* done, float* positions);
 oct_status oct_server_get_stats(oct_server* srv, oct_server_stats* out);
 oct_status oct_server_destroy(oct_server* srv);
+
+/* VTK 5.1 ASCII unstructured grids, one element type (VTK_Formater::save_mesh and
+ * add_scalar_data / add_vector_data, octopus/src/Mesh/Converter/VTK_Formater.cpp; VTK_Loader::load
+ * and get_point_data_v3, octopus/src/Mesh/Converter/MeshLoader.cpp:97-330).  The text matches the
+ * reference writer's byte for byte; Hexa27 nodes go to and come from VTK's node order. */
+enum { OCT_VTK_POINT = 0, OCT_VTK_CELL = 1 };
+typedef struct oct_vtk_field {
+    const char* name;
+    int32_t location;      /* OCT_VTK_POINT (n_nodes values) or OCT_VTK_CELL (n_elements values) */
+    int32_t components;    /* 1: SCALARS, 3: VECTORS */
+    const float* data;
+} oct_vtk_field;
+oct_status oct_vtk_write(const char* path, const float* positions, int32_t n_nodes, int32_t element,
+                         const int32_t* topology, int32_t n_elements, const oct_vtk_field* fields, int32_t n_fields);
+/* Reads a mesh; with positions and topology NULL only the sizes and element type are set.
+ * OCT_ENOTSUP for binary files, other datasets or mixed element types. */
+oct_status oct_vtk_read_mesh(const char* path, int32_t* element, int32_t* n_nodes, int32_t* n_elements, float* positions,
+                             int32_t* topology);
+/* Reads n values of the named SCALARS (components 1) or VECTORS (components 3) field. */
+oct_status oct_vtk_read_field(const char* path, const char* name, int32_t components, int32_t n, float* out);
+/* One frame of FEM_VTK_Recorder::save (octopus/src/Script/Record/Recorder.cpp:117-171): rest mesh,
+ * point data weights (masses), u_norm, u (displacement), smooth_stress; cell data stress
+ * (OCT_DIAG_STRESS_ACCUMULATED), volume, volume_diff, inverted.  The reference's recorder writes
+ * the inversion flags under volume_diff and zeros under inverted; here both hold their values. */
+oct_status oct_scene_write_vtk(oct_scene* s, const char* path);
+
+/* Shape-function values N (nodes of the element) at reference coordinates x
+ * (FEM_Shape::build_shape, octopus/include/Dynamic/FEM/FEM_Shape.h) and the reference-element
+ * node coordinates (3 per node; FEM_Shape::get_vertices for the corners). */
+oct_status oct_shape_values(int32_t element, const double x[3], double* N);
+oct_status oct_reference_nodes(int32_t element, double* X);
+
+/* Accuracy measures of the reference's experiments (octopus/include/Script/Measure/MeshDiff.h,
+ * octopus/src/Script/Record/Recorder.cpp:190-330); errors accumulated in FP64.
+ * out6 = {MSE, RMSE, MAE, max, L1, L2} of the per-point error vectors (Error::update). */
+/* MeshDiff_MSE: e_i = a_i - b_i - offset (offset may be NULL). */
+oct_status oct_mesh_error(const float* a, const float* b, int32_t n, const float offset[3], double out6[6]);
+/* Beam_MSE_Sampling: a regular grid of samples (nb_sample per unit length) inside the
+ * reference mesh's box is located, at rest, in an element of every mesh; the error of mesh m
+ * compares the samples interpolated in its current positions and in the reference mesh's,
+ * each relative to its rest box minimum.  Samples some mesh does not contain are dropped. */
+typedef struct oct_sampler oct_sampler;
+oct_status oct_beam_sampler_create(int32_t n_meshes, const int32_t* elements, const int32_t* n_nodes,
+                                   const float* const* rest_positions, const int32_t* n_elements,
+                                   const int32_t* const* topologies, int32_t reference, int32_t nb_sample, oct_sampler** out);
+oct_status oct_beam_sampler_info(oct_sampler* s, int32_t* n_samples);
+oct_status oct_beam_sampler_error(oct_sampler* s, int32_t mesh, const float* positions, const float* reference_positions,
+                                  double out6[6]);
+oct_status oct_beam_sampler_destroy(oct_sampler* s);
+/* FEM_Flexion_error_recorder: |target - p|^2 of the first particle whose rest position is
+ * within 1e-3 of follow; its index in *particle (may be NULL). */
+oct_status oct_flexion_error(const float* rest, const float* current, int32_t n, const float follow[3], const float target[3],
+                             double* error, int32_t* particle);
+/* FEM_Torsion_error_recorder: samples_per_edge points on every element edge lying on the beam's
+ * y = z = 0 edge; for each, the rotation angle (degrees) about the section centre (0.5, 0.5)
+ * between rest and current state, against its current x / beam_length; sorted by distance,
+ * points closer than 1e-4 merged (angles averaged).  *count = number of points (the arrays
+ * receive at most capacity). */
+oct_status oct_torsion_profile(int32_t element, const float* rest, const float* current, int32_t n_nodes,
+                               const int32_t* topology, int32_t n_elements, int32_t samples_per_edge, float beam_length,
+                               float* distance, float* angles, int32_t capacity, int32_t* count);
 
 /* Measurement helpers.  The context's CUDA stream (cudaStream_t), to record events on it. */
 oct_status oct_ctx_stream(oct_ctx* ctx, void** stream);

@@ -23,9 +23,10 @@ from .capi import (COLOR_DSAT, COLOR_GREEDY, COROTATED, ELEMENT_NODES, FIXED_COR
                    MASS_FEMSHAPE, MASS_UNIFORM, NEOHOOKE, ORDER_ASCENDING, ORDER_SHUFFLED, PREC_MIXED, PREC_PLAIN,
                    SOLVER_EXPLICIT, SOLVER_VBD, SOLVER_XPBD, STABLE_NEOHOOKE, STVK, TETRA, TETRA10, TETRA20, VBD_BASE,
                    VBD_BETTER_COLORATION, VBD_REDUCTION_SYMMETRY, XPBD_OPTIGROUP, XPBD_OPTISHARED, XPBD_QUADRATURE,
-                   XPBD_XPBD, OctError, beam_mesh, color, fixed_by_plane, lumped_masses, shape_table)
+                   XPBD_XPBD, OctError, beam_mesh, color, fixed_by_plane, lumped_masses, shape_table, vtk_read,
+                   vtk_read_field, vtk_write)
 
-__all__ = ["Context", "Scene", "Batch", "Server", "make_desc", "autotune_mapping", "OctError", "beam_mesh", "color", "lumped_masses", "shape_table",
+__all__ = ["Context", "Scene", "Batch", "Server", "make_desc", "autotune_mapping", "vtk_read", "vtk_read_field", "vtk_write", "OctError", "beam_mesh", "color", "lumped_masses", "shape_table",
            "fixed_by_plane", "library_path"]
 
 
@@ -189,6 +190,24 @@ class Scene:
         capi.check(capi.lib().oct_scene_energy(self._h, capi.ptr(e, C.c_double)), "oct_scene_energy",
                    self.ctx.handle)
         return e
+
+    def write_vtk(self, path):
+        """One FEM_VTK_Recorder frame of this scene (oct_scene_write_vtk)."""
+        capi.check(capi.lib().oct_scene_write_vtk(self._h, path.encode()), "oct_scene_write_vtk", self.ctx.handle)
+
+    def metadata(self):
+        """Run metadata (mesh counts, material) as the reference's recorders write it, parsed."""
+        import json
+        n = C.c_size_t()
+        capi.check(capi.lib().oct_scene_metadata_json(self._h, None, 0, C.byref(n)), "oct_scene_metadata_json")
+        buf = C.create_string_buffer(n.value + 1)
+        capi.check(capi.lib().oct_scene_metadata_json(self._h, buf, n.value + 1, C.byref(n)), "oct_scene_metadata_json")
+        return json.loads(buf.value.decode())
+
+    def topology(self):
+        out = np.zeros((self.n_elements, ELEMENT_NODES[self.element]), np.int32)
+        capi.check(capi.lib().oct_scene_get_topology(self._h, capi.ptr(out, C.c_int32)), "oct_scene_get_topology")
+        return out
 
     def element_data(self, kind):
         """Per-element diagnostic (capi.DIAG_STRESS / VOLUME / VOLUME_DIFF / INVERTED)."""

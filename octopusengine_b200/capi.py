@@ -40,8 +40,18 @@ EXPORTS = [
     "oct_server_create", "oct_server_submit", "oct_server_tick", "oct_server_poll", "oct_server_get_stats",
     "oct_server_destroy", "oct_elastic_energy_noalloc", "oct_scene_set_fixation_group",
     "oct_scene_element_data", "oct_scene_vertex_residuals", "oct_scene_set_mapping", "oct_autotune_mapping",
-    "oct_batch_prepare",
+    "oct_batch_prepare", "oct_scene_element_type", "oct_scene_get_rest_positions", "oct_scene_get_topology",
+    "oct_scene_metadata_json", "oct_vtk_write", "oct_vtk_read_mesh", "oct_vtk_read_field", "oct_scene_write_vtk",
+    "oct_shape_values", "oct_reference_nodes", "oct_mesh_error", "oct_beam_sampler_create", "oct_beam_sampler_info",
+    "oct_beam_sampler_error", "oct_beam_sampler_destroy", "oct_flexion_error", "oct_torsion_profile",
 ]
+
+
+class VtkField(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("location", C.c_int32), ("components", C.c_int32), ("data", C.POINTER(C.c_float))]
+
+
+VTK_POINT, VTK_CELL = 0, 1
 
 
 class ServerConfig(C.Structure):
@@ -105,6 +115,32 @@ def lib():
             "oct_scene_element_data": ([vp, C.c_int, C.POINTER(C.c_float)], C.c_int),
             "oct_scene_set_mapping": ([vp, C.c_int], C.c_int),
             "oct_batch_prepare": ([vp, C.c_float, C.c_int], C.c_int),
+            "oct_scene_element_type": ([vp, C.POINTER(C.c_int32)], C.c_int),
+            "oct_scene_get_rest_positions": ([vp, C.POINTER(C.c_float)], C.c_int),
+            "oct_scene_get_topology": ([vp, C.POINTER(C.c_int32)], C.c_int),
+            "oct_scene_metadata_json": ([vp, C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)], C.c_int),
+            "oct_vtk_write": ([C.c_char_p, C.POINTER(C.c_float), C.c_int32, C.c_int32, C.POINTER(C.c_int32), C.c_int32,
+                               C.POINTER(VtkField), C.c_int32], C.c_int),
+            "oct_vtk_read_mesh": ([C.c_char_p, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                   C.POINTER(C.c_float), C.POINTER(C.c_int32)], C.c_int),
+            "oct_vtk_read_field": ([C.c_char_p, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(C.c_float)], C.c_int),
+            "oct_scene_write_vtk": ([vp, C.c_char_p], C.c_int),
+            "oct_shape_values": ([C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+            "oct_reference_nodes": ([C.c_int32, C.POINTER(C.c_double)], C.c_int),
+            "oct_mesh_error": ([C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_float),
+                                C.POINTER(C.c_double)], C.c_int),
+            "oct_beam_sampler_create": ([C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.POINTER(C.c_float)),
+                                         C.POINTER(C.c_int32), C.POINTER(C.POINTER(C.c_int32)), C.c_int32, C.c_int32,
+                                         C.POINTER(vp)], C.c_int),
+            "oct_beam_sampler_info": ([vp, C.POINTER(C.c_int32)], C.c_int),
+            "oct_beam_sampler_error": ([vp, C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_double)],
+                                       C.c_int),
+            "oct_beam_sampler_destroy": ([vp], C.c_int),
+            "oct_flexion_error": ([C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float), C.POINTER(C.c_double), C.POINTER(C.c_int32)], C.c_int),
+            "oct_torsion_profile": ([C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_int32),
+                                     C.c_int32, C.c_int32, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32,
+                                     C.POINTER(C.c_int32)], C.c_int),
             "oct_autotune_mapping": ([vp, C.POINTER(vp), C.c_int, C.c_float, C.c_int, C.POINTER(C.c_int32)], C.c_int),
             "oct_scene_vertex_residuals": ([vp, C.c_float, C.POINTER(C.c_float)], C.c_int),
             "oct_scene_get_positions": ([vp, fp], C.c_int),
@@ -181,6 +217,128 @@ def beam_mesh(element, cells, size, offset=(0.0, 0.0, 0.0)):
     check(L.oct_beam_mesh(element, cells[0], cells[1], cells[2], ptr(sz, C.c_float), ptr(off, C.c_float),
                           C.byref(nn), C.byref(ne), ptr(X, C.c_float), ptr(T, C.c_int32)), "oct_beam_mesh")
     return X, T
+
+
+def vtk_write(path, element, X, T, point_fields=(), cell_fields=()):
+    """VTK 5.1 ASCII file of one mesh; fields are (name, array) with 1 or 3 values per point/cell."""
+    X = np.ascontiguousarray(X, np.float32)
+    T = np.ascontiguousarray(T, np.int32)
+    keep, fs = [], []
+    for loc, group in ((VTK_POINT, point_fields), (VTK_CELL, cell_fields)):
+        for name, a in group:
+            a = np.ascontiguousarray(a, np.float32)
+            keep.append(a)
+            comps = 3 if a.ndim == 2 and a.shape[1] == 3 else 1
+            fs.append(VtkField(name.encode(), loc, comps, ptr(a, C.c_float)))
+    arr = (VtkField * max(len(fs), 1))(*fs)
+    check(lib().oct_vtk_write(path.encode(), ptr(X, C.c_float), len(X), element, ptr(T, C.c_int32), len(T), arr, len(fs)),
+          "oct_vtk_write")
+
+
+def vtk_read(path):
+    """(element, X, T) of a VTK 5.1 ASCII unstructured grid with one element type."""
+    e, nn, ne = C.c_int32(), C.c_int32(), C.c_int32()
+    check(lib().oct_vtk_read_mesh(path.encode(), C.byref(e), C.byref(nn), C.byref(ne), None, None), "oct_vtk_read_mesh")
+    X = np.zeros((nn.value, 3), np.float32)
+    T = np.zeros((ne.value, ELEMENT_NODES.get(e.value, 1)), np.int32)
+    check(lib().oct_vtk_read_mesh(path.encode(), C.byref(e), C.byref(nn), C.byref(ne), ptr(X, C.c_float),
+                                  ptr(T, C.c_int32)), "oct_vtk_read_mesh")
+    return e.value, X, T
+
+
+def vtk_read_field(path, name, n, components=1):
+    out = np.zeros((n, components) if components == 3 else n, np.float32)
+    check(lib().oct_vtk_read_field(path.encode(), name.encode(), components, n, ptr(out, C.c_float)), "oct_vtk_read_field")
+    return out
+
+
+ERROR_KEYS = ("MSE", "RMSE", "MAE", "max", "L1", "L2")
+
+
+def shape_values(element, x):
+    N = np.zeros(ELEMENT_NODES[element])
+    xx = np.ascontiguousarray(x, np.float64)
+    check(lib().oct_shape_values(element, ptr(xx, C.c_double), ptr(N, C.c_double)), "oct_shape_values")
+    return N
+
+
+def reference_nodes(element):
+    X = np.zeros((ELEMENT_NODES[element], 3))
+    check(lib().oct_reference_nodes(element, ptr(X, C.c_double)), "oct_reference_nodes")
+    return X
+
+
+def mesh_error(a, b, offset=None):
+    """MeshDiff_MSE error between two same-topology node sets: dict MSE, RMSE, MAE, max, L1, L2."""
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    out = np.zeros(6)
+    off = None if offset is None else np.ascontiguousarray(offset, np.float32)
+    check(lib().oct_mesh_error(ptr(a, C.c_float), ptr(b, C.c_float), len(a), ptr(off, C.c_float) if off is not None else None,
+                               ptr(out, C.c_double)), "oct_mesh_error")
+    return dict(zip(ERROR_KEYS, out))
+
+
+class BeamSampler:
+    """Beam_MSE_Sampling over meshes [(element, rest X, T), ...] against meshes[reference]."""
+
+    def __init__(self, meshes, reference=0, nb_sample=4):
+        self._keep = [(np.ascontiguousarray(X, np.float32), np.ascontiguousarray(T, np.int32)) for _, X, T in meshes]
+        n = len(meshes)
+        el = (C.c_int32 * n)(*[e for e, _, _ in meshes])
+        nn = (C.c_int32 * n)(*[len(X) for X, _ in self._keep])
+        ne = (C.c_int32 * n)(*[len(T) for _, T in self._keep])
+        xs = (C.POINTER(C.c_float) * n)(*[ptr(X, C.c_float) for X, _ in self._keep])
+        ts = (C.POINTER(C.c_int32) * n)(*[ptr(T, C.c_int32) for _, T in self._keep])
+        self._h = C.c_void_p()
+        check(lib().oct_beam_sampler_create(n, el, nn, xs, ne, ts, reference, nb_sample, C.byref(self._h)),
+              "oct_beam_sampler_create")
+        k = C.c_int32()
+        lib().oct_beam_sampler_info(self._h, C.byref(k))
+        self.n_samples = k.value
+
+    def error(self, mesh, positions, reference_positions):
+        p = np.ascontiguousarray(positions, np.float32)
+        r = np.ascontiguousarray(reference_positions, np.float32)
+        out = np.zeros(6)
+        check(lib().oct_beam_sampler_error(self._h, mesh, ptr(p, C.c_float), ptr(r, C.c_float), ptr(out, C.c_double)),
+              "oct_beam_sampler_error")
+        return dict(zip(ERROR_KEYS, out))
+
+    def close(self):
+        if self._h:
+            lib().oct_beam_sampler_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def flexion_error(rest, current, follow, target):
+    rest = np.ascontiguousarray(rest, np.float32)
+    cur = np.ascontiguousarray(current, np.float32)
+    f = np.ascontiguousarray(follow, np.float32)
+    t = np.ascontiguousarray(target, np.float32)
+    err, pid = C.c_double(), C.c_int32()
+    check(lib().oct_flexion_error(ptr(rest, C.c_float), ptr(cur, C.c_float), len(rest), ptr(f, C.c_float),
+                                  ptr(t, C.c_float), C.byref(err), C.byref(pid)), "oct_flexion_error")
+    return err.value, pid.value
+
+
+def torsion_profile(element, rest, current, T, samples_per_edge, beam_length):
+    rest = np.ascontiguousarray(rest, np.float32)
+    cur = np.ascontiguousarray(current, np.float32)
+    T = np.ascontiguousarray(T, np.int32)
+    n = C.c_int32()
+    args = (element, ptr(rest, C.c_float), ptr(cur, C.c_float), len(rest), ptr(T, C.c_int32), len(T), samples_per_edge,
+            beam_length)
+    check(lib().oct_torsion_profile(*args, None, None, 0, C.byref(n)), "oct_torsion_profile")
+    d, a = np.zeros(n.value, np.float32), np.zeros(n.value, np.float32)
+    check(lib().oct_torsion_profile(*args, ptr(d, C.c_float), ptr(a, C.c_float), n.value, C.byref(n)), "oct_torsion_profile")
+    return d, a
 
 
 def lumped_masses(element, X, T, density, distribution=MASS_FEMSHAPE):

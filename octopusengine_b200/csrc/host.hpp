@@ -23,6 +23,10 @@ struct ShapeTable {
     std::vector<double> dN;   // (q * ne + i) * 3 + k
 };
 bool shape_table(int element, ShapeTable& out);
+// Shape-function values at reference coordinates x[3] (N: nodes of the element) and the
+// reference-element node coordinates (X: 3 per node).
+bool shape_values(int element, const double* x, double* N);
+bool reference_nodes(int element, double* X);
 
 // Beam meshes as BeamMeshGenerator builds them (octopus/src/Mesh/Generator/BeamGenerator.cpp):
 // hex grid of nx*ny*nz cells over size sx*sy*sz at an offset; tetra elements use the 6-tet

@@ -11,6 +11,7 @@
 #include <mutex>
 #include <numeric>
 #include <random>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -90,6 +91,8 @@ struct oct_scene {
     int n_nodes = 0, n_elements = 0, n_fixed = 0, n_colors = 0;
     int iterations = 1, order_mode = 0, tpv = 8, precision = 0, max_valence = 0;
     float rho = 0.f, global_damping = 0.f;
+    float young = 0.f, poisson = 0.f, density = 0.f;   // as described (run metadata)
+    int last_substeps = 0;
     bool in_place = true, box = false, has_v0 = false;
     bool xpbd_raw = true, xpbd_project = true;   // XPBD update form; false: no projection (OptiGroup)
     // frame graph (oct_scene_set_capture): the sub-steps of one frame, replayed while the
@@ -251,6 +254,9 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     s->solver = d->solver;
     s->element = d->element;
     s->material = d->material;
+    s->young = d->young;
+    s->poisson = d->poisson;
+    s->density = d->density;
     s->ne = element_nodes(d->element);
     s->nq = element_quadrature(d->element);
     if (s->ne < 0) return fail(c, OCT_EINVAL, "unsupported element type");
@@ -751,6 +757,7 @@ oct_status oct_scene_step(oct_scene* s, float frame_dt, int substeps) {
     if (!s || substeps <= 0 || !(frame_dt > 0.f)) return OCT_EINVAL;
     oct_ctx* c = s->ctx;
     const float sub = frame_dt / (float)substeps;
+    s->last_substeps = substeps;
     // the first frame after set-up (pending initial velocity) and shuffled colour orders run
     // launch by launch; otherwise a captured frame is replayed
     const bool graph = s->capture && s->order_mode != OCT_ORDER_SHUFFLED && !s->pending_host;
@@ -840,6 +847,45 @@ oct_status oct_scene_get_coloring(oct_scene* s, int32_t* colors, int32_t* order)
     if (!s) return OCT_EINVAL;
     if (colors) std::copy(s->colors.begin(), s->colors.end(), colors);
     if (order) std::copy(s->vids.begin(), s->vids.end(), order);
+    return OCT_OK;
+}
+
+oct_status oct_scene_element_type(oct_scene* s, int32_t* element) {
+    if (!s || !element) return OCT_EINVAL;
+    *element = s->element;
+    return OCT_OK;
+}
+
+oct_status oct_scene_get_rest_positions(oct_scene* s, float* out) {
+    if (!s || !out) return OCT_EINVAL;
+    std::copy(s->X.begin(), s->X.end(), out);
+    return OCT_OK;
+}
+
+oct_status oct_scene_get_topology(oct_scene* s, int32_t* out) {
+    if (!s || !out) return OCT_EINVAL;
+    OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    OCT_CUDA(s->ctx, cudaMemcpy(out, s->h.topo, sizeof(int32_t) * (size_t)s->n_elements * s->ne, cudaMemcpyDeviceToHost));
+    return OCT_OK;
+}
+
+// Run metadata as the reference's recorders write it into their JSON (MeshRecorder and
+// FEM_Dynamic_Recorder::add_data_json, octopus/src/Script/Record/Recorder.cpp:12-36), the two
+// objects under "mesh" and "fem"; numbers in the same default stream formatting.
+oct_status oct_scene_metadata_json(oct_scene* s, char* out, size_t capacity, size_t* length) {
+    if (!s) return OCT_EINVAL;
+    static const char* elem_names[10] = {"Line", "Triangle", "Quad", "Tetra", "Pyramid", "Prism", "Hexa", "Tetra10",
+                                         "Tetra20", "Hexa27"};
+    static const char* mat_names[6] = {"Hooke", "SaintVenant", "Neo-Hooke", "Stable Neo-Hooke", "", ""};
+    std::ostringstream j;
+    j << "{\"mesh\" : {\"" << elem_names[s->element] << "\" : " << s->n_elements << ",\"vertices\" : " << s->n_nodes << "},"
+      << "\"fem\" : {\"material\" : \"" << mat_names[s->material] << "\",\"poisson\" : " << s->poisson
+      << ",\"young\" : " << s->young << ",\"sub_step\" : " << s->last_substeps << ",\"density\" : " << s->density << "}}";
+    const std::string str = j.str();
+    if (length) *length = str.size();
+    if (!out) return OCT_OK;
+    if (capacity < str.size() + 1) return fail(s->ctx, OCT_EINVAL, "metadata buffer too small");
+    std::memcpy(out, str.c_str(), str.size() + 1);
     return OCT_OK;
 }
 

@@ -129,6 +129,64 @@ void hex_derivatives(int e, const double* x, double* dN) {
 
 }  // namespace
 
+// Shape-function values at reference coordinates x (FEM_Shape::build_shape), same bases as
+// the derivatives above.
+bool shape_values(int e, const double* x, double* N) {
+    if (e == kTetra || e == kTetra10 || e == kTetra20) {
+        const double L[4] = {1.0 - x[0] - x[1] - x[2], x[0], x[1], x[2]};
+        if (e == kTetra) {
+            for (int i = 0; i < 4; ++i) N[i] = L[i];
+        } else if (e == kTetra10) {
+            for (int i = 0; i < 4; ++i) N[i] = L[i] * (2.0 * L[i] - 1.0);
+            for (int k = 0; k < 6; ++k) N[4 + k] = 4.0 * L[kP2Edges[k][0]] * L[kP2Edges[k][1]];
+        } else {
+            for (int i = 0; i < 4; ++i) N[i] = 0.5 * (3.0 * L[i] - 1.0) * (3.0 * L[i] - 2.0) * L[i];
+            for (int k = 0; k < 12; ++k) {
+                const double li = L[kP3Edges[k][0]], lj = L[kP3Edges[k][1]];
+                N[4 + k] = 4.5 * li * lj * (3.0 * li - 1.0);
+            }
+            for (int k = 0; k < 4; ++k) N[16 + k] = 27.0 * L[kP3Faces[k][0]] * L[kP3Faces[k][1]] * L[kP3Faces[k][2]];
+        }
+        return true;
+    }
+    if (e == kHexa || e == kHexa27) {
+        const int ne = e == kHexa ? 8 : 27;
+        for (int i = 0; i < ne; ++i) {
+            const int* n = kHexNodes[i];
+            N[i] = e == kHexa ? 0.125 * (1.0 + n[0] * x[0]) * (1.0 + n[1] * x[1]) * (1.0 + n[2] * x[2])
+                              : lag(n[0], x[0]) * lag(n[1], x[1]) * lag(n[2], x[2]);
+        }
+        return true;
+    }
+    return false;
+}
+
+// Reference-element node coordinates (FEM_Shape::get_vertices for the corners; edge and face
+// nodes where the node tables put them).
+bool reference_nodes(int e, double* X) {
+    const double tc[4][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    auto put = [&](int node, double a, int i, double b, int j, double c = 0, int k = 0) {
+        for (int d = 0; d < 3; ++d) X[3 * node + d] = a * tc[i][d] + b * tc[j][d] + c * tc[k][d];
+    };
+    if (e == kTetra || e == kTetra10 || e == kTetra20) {
+        for (int i = 0; i < 4; ++i) put(i, 1.0, i, 0.0, i);
+        if (e == kTetra10)
+            for (int k = 0; k < 6; ++k) put(4 + k, 0.5, kP2Edges[k][0], 0.5, kP2Edges[k][1]);
+        if (e == kTetra20) {
+            for (int k = 0; k < 12; ++k) put(4 + k, 2.0 / 3.0, kP3Edges[k][0], 1.0 / 3.0, kP3Edges[k][1]);
+            for (int k = 0; k < 4; ++k) put(16 + k, 1.0 / 3.0, kP3Faces[k][0], 1.0 / 3.0, kP3Faces[k][1], 1.0 / 3.0, kP3Faces[k][2]);
+        }
+        return true;
+    }
+    if (e == kHexa || e == kHexa27) {
+        const int ne = e == kHexa ? 8 : 27;
+        for (int i = 0; i < ne; ++i)
+            for (int d = 0; d < 3; ++d) X[3 * i + d] = kHexNodes[i][d];
+        return true;
+    }
+    return false;
+}
+
 bool shape_table(int e, ShapeTable& s) {
     s = ShapeTable();
     s.ne = element_nodes(e);

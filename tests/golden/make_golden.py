@@ -227,6 +227,11 @@ def extract_meshes():
                 topo += [cell[HEXA27_VTK_SWAP.get(k, k)] for k in range(27)]
         import struct
         blob = struct.pack("<%di" % len(topo), *topo)
+        text = open(os.path.join(d, fname), "rb").read()
+        a = text.index(b"DATASET UNSTRUCTURED_GRID")
+        b = text.index(b"POINT_DATA")
+        c = text.index(b"SCALARS weights float 1")
+        e = text.index(b"\n", text.index(b"LOOKUP_TABLE default", c) + 21) + 1   # end of the values line
         step = 97
         out[elem] = {
             "source": "assets/result/vtk/References/" + fname,
@@ -239,6 +244,10 @@ def extract_meshes():
             "points_sample": pts[::step],
             "mass_sample": weights[::step],
             "mass_sum": sum(weights),
+            # the reference's own VTK text (VTK_Formater::save_mesh and the masses block of
+            # FEM_VTK_Recorder::save): a writer with the same formatting reproduces it byte for byte
+            "mesh_text_sha256": hashlib.sha256(text[a:b]).hexdigest(),
+            "weights_text_sha256": hashlib.sha256(text[c:e]).hexdigest(),
         }
     return out
 
