@@ -160,6 +160,28 @@ oct_status oct_scene_set_fixation_group(oct_scene* s, int group, const float off
 /* Switches the scene between OCT_PREC_PLAIN and OCT_PREC_MIXED for its own steps (a batch
  * keeps the precision its scenes had when the batch was created). */
 oct_status oct_scene_set_precision(oct_scene* s, int precision);
+/* Scripted effects of the reference's rigid controller (Cuda_Constraint_Rigid_Controller,
+ * octopus/src/Script/Dynamic/Cuda_Constraint_Rigid_Controller.cpp:9-23; GPU_Crush,
+ * GPU_RandomSphere, GPU_HighStretch, octopus/include/GPU/GPU_Constraint.h:20-80, kernels
+ * octopus/src/GPU/GPU_Constraint.cu:22-92):
+ *   OCT_EFFECT_CRUSH          free nodes flattened to y = 0 (velocity 0)
+ *   OCT_EFFECT_RANDOM_SPHERE  free nodes scattered in a sphere of radius params[0] about the
+ *                             node centroid by the reference's sine hash
+ *   OCT_EFFECT_HIGH_STRETCH   params[0] boundary nodes chosen farthest-first are pushed away
+ *                             from the centroid by t, t growing by dt per call up to params[1]
+ * Effects are created inactive (as the controller creates them) and run, while active, after
+ * the fixation and before the box limit, in creation order, wherever the constraints run (every
+ * VBD iteration; every XPBD or explicit sub-step).  At most 4 per scene; add them before the
+ * scene joins a batch (the batch's graph is captured with the effects it finds); toggling works
+ * at any time. */
+enum { OCT_EFFECT_CRUSH = 0, OCT_EFFECT_RANDOM_SPHERE = 1, OCT_EFFECT_HIGH_STRETCH = 2 };
+oct_status oct_scene_add_effect(oct_scene* s, int kind, const float* params, int32_t* index);
+oct_status oct_scene_set_effect_active(oct_scene* s, int32_t index, int active);
+/* The node ids a high-stretch effect moves (n = 0 for the other kinds). */
+oct_status oct_scene_effect_ids(oct_scene* s, int32_t index, int32_t* ids, int32_t* n);
+/* Boundary nodes of a mesh, ascending (MeshTools::Get_Surface_Geometry_Ids,
+ * octopus/include/Mesh/MeshTools.h:64-89); ids may be NULL to get the count. */
+oct_status oct_surface_nodes(int32_t element, const int32_t* topology, int32_t n_elements, int32_t* ids, int32_t* n);
 /* FP64 diagnostics: kinetic, elastic, gravity potential, total energy; and the VBD
  * residual r = f - M/dt^2 (p - y) - damping term (kernel_vbd_compute_residual) as
  * [sum |r|, max |r|] over free nodes.  Both return OCT_ENUMERIC on NaN/Inf state. */

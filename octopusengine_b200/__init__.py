@@ -191,6 +191,26 @@ class Scene:
                    self.ctx.handle)
         return e
 
+    def add_effect(self, kind, *params):
+        """Scripted effect (capi.EFFECT_*), created inactive; returns its index."""
+        idx = C.c_int32()
+        p = np.asarray(params if params else [0.0], np.float32)
+        capi.check(capi.lib().oct_scene_add_effect(self._h, kind, capi.ptr(p, C.c_float), C.byref(idx)),
+                   "oct_scene_add_effect", self.ctx.handle)
+        return idx.value
+
+    def set_effect_active(self, index, active=True):
+        capi.check(capi.lib().oct_scene_set_effect_active(self._h, index, int(active)), "oct_scene_set_effect_active",
+                   self.ctx.handle)
+
+    def effect_ids(self, index):
+        n = C.c_int32()
+        capi.check(capi.lib().oct_scene_effect_ids(self._h, index, None, C.byref(n)), "oct_scene_effect_ids")
+        out = np.zeros(n.value, np.int32)
+        capi.check(capi.lib().oct_scene_effect_ids(self._h, index, capi.ptr(out, C.c_int32), C.byref(n)),
+                   "oct_scene_effect_ids")
+        return out
+
     def write_vtk(self, path):
         """One FEM_VTK_Recorder frame of this scene (oct_scene_write_vtk)."""
         capi.check(capi.lib().oct_scene_write_vtk(self._h, path.encode()), "oct_scene_write_vtk", self.ctx.handle)

@@ -20,6 +20,7 @@ ELEMENT_QUADRATURE = {TETRA: 1, HEXA: 8, TETRA10: 4, TETRA20: 11, HEXA27: 27}
 HOOKE, STVK, NEOHOOKE, STABLE_NEOHOOKE, COROTATED, FIXED_COROTATED = 0, 1, 2, 3, 4, 5
 XPBD_XPBD, XPBD_QUADRATURE, XPBD_OPTISHARED, XPBD_OPTIGROUP = 0, 1, 2, 3
 DIAG_STRESS, DIAG_VOLUME, DIAG_VOLUME_DIFF, DIAG_INVERTED, DIAG_STRESS_ACCUMULATED = 0, 1, 2, 3, 4
+EFFECT_CRUSH, EFFECT_RANDOM_SPHERE, EFFECT_HIGH_STRETCH = 0, 1, 2
 MASS_UNIFORM, MASS_FEMSHAPE = 0, 1
 SOLVER_VBD, SOLVER_XPBD, SOLVER_EXPLICIT = 0, 1, 2
 VBD_BASE, VBD_THREADED_QUADRATURE, VBD_REDUCTION_SYMMETRY, VBD_BETTER_COLORATION = 0, 1, 2, 3
@@ -44,6 +45,7 @@ EXPORTS = [
     "oct_scene_metadata_json", "oct_vtk_write", "oct_vtk_read_mesh", "oct_vtk_read_field", "oct_scene_write_vtk",
     "oct_shape_values", "oct_reference_nodes", "oct_mesh_error", "oct_beam_sampler_create", "oct_beam_sampler_info",
     "oct_beam_sampler_error", "oct_beam_sampler_destroy", "oct_flexion_error", "oct_torsion_profile",
+    "oct_scene_add_effect", "oct_scene_set_effect_active", "oct_scene_effect_ids", "oct_surface_nodes",
 ]
 
 
@@ -126,6 +128,11 @@ def lib():
             "oct_vtk_read_field": ([C.c_char_p, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(C.c_float)], C.c_int),
             "oct_scene_write_vtk": ([vp, C.c_char_p], C.c_int),
             "oct_shape_values": ([C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+            "oct_scene_add_effect": ([vp, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int32)], C.c_int),
+            "oct_scene_set_effect_active": ([vp, C.c_int32, C.c_int], C.c_int),
+            "oct_scene_effect_ids": ([vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
+            "oct_surface_nodes": ([C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],
+                                  C.c_int),
             "oct_reference_nodes": ([C.c_int32, C.POINTER(C.c_double)], C.c_int),
             "oct_mesh_error": ([C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int32, C.POINTER(C.c_float),
                                 C.POINTER(C.c_double)], C.c_int),
@@ -217,6 +224,15 @@ def beam_mesh(element, cells, size, offset=(0.0, 0.0, 0.0)):
     check(L.oct_beam_mesh(element, cells[0], cells[1], cells[2], ptr(sz, C.c_float), ptr(off, C.c_float),
                           C.byref(nn), C.byref(ne), ptr(X, C.c_float), ptr(T, C.c_int32)), "oct_beam_mesh")
     return X, T
+
+
+def surface_nodes(element, T):
+    T = np.ascontiguousarray(T, np.int32)
+    n = C.c_int32()
+    check(lib().oct_surface_nodes(element, ptr(T, C.c_int32), len(T), None, C.byref(n)), "oct_surface_nodes")
+    out = np.zeros(n.value, np.int32)
+    check(lib().oct_surface_nodes(element, ptr(T, C.c_int32), len(T), ptr(out, C.c_int32), C.byref(n)), "oct_surface_nodes")
+    return out
 
 
 def vtk_write(path, element, X, T, point_fields=(), cell_fields=()):

@@ -29,6 +29,24 @@ constexpr int kMaxNE = 27;
 constexpr int kMaxNQ = 27;
 constexpr int kOwnerShift = 5;
 constexpr int kFixGroups = 4;
+constexpr int kMaxEffects = 4;
+
+// Scripted constraint effects of the reference's rigid controller (GPU_Crush, GPU_RandomSphere,
+// GPU_HighStretch; octopus/include/GPU/GPU_Constraint.h:20-80).  kind < 0: unused slot.  The
+// active flag and the stretch distance t live on the device so that toggling an effect does
+// not invalidate captured graphs.
+struct EffectDev {
+    int kind;           // 0 crush, 1 random sphere, 2 high stretch
+    int active;
+    int n;              // high stretch: number of ids
+    int pad;
+    const int* ids;     // high stretch: the stretched node ids
+    float* t;           // high stretch: current distance (device)
+    float cx, cy, cz;   // centre
+    float radius;       // random sphere
+    float max_dist;     // high stretch
+    float pad2[3];
+};
 
 struct SceneDev {
     float4* u;          // displacement, per node
@@ -56,6 +74,7 @@ struct SceneDev {
     float bminx, bminy, bminz, bmaxx, bmaxy, bmaxz;
     int box_limit;
     int precision;                     // 0 plain, 1 mixed
+    EffectDev* effects;                // kMaxEffects slots (scene memory)
 };
 
 // One unit of colour work: `count` consecutive colour slots of one scene.  With a fixed

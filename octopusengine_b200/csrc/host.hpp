@@ -35,6 +35,8 @@ bool beam_mesh(int element, int nx, int ny, int nz, float sx, float sy, float sz
                std::vector<float>& X, std::vector<int32_t>& topo);
 
 // compute_fem_mass (octopus/src/Dynamic/FEM/FEM_Shape.cpp:86-121).
+// Boundary nodes of a mesh, ascending (MeshTools::Get_Surface_Geometry_Ids).
+std::vector<int32_t> surface_nodes(int element, const int32_t* topo, int n_elements);
 void lumped_masses(int element, const float* X, int n_nodes, const int32_t* topo, int n_elements, float density,
                    int distribution, std::vector<float>& mass);
 

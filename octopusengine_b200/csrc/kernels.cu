@@ -692,6 +692,68 @@ __global__ void k_constraints(const SceneDev* __restrict__ scenes, const NWork* 
     }
 }
 
+// Scripted effects (GPU_Constraint.cu:22-92), run after the fixation in creation order.
+//   crush (kernel_constraint_crush): free nodes flattened to y = 0, last position = position,
+//     velocity 0
+//   random sphere (kernel_constraint_random_sphere): free nodes scattered inside a sphere by
+//     the sine hash fract(sin(v) * k) of the reference, last position = position, velocity 0
+//   high stretch (kernel_constraint_high_stretch): t = min(t + dt, max_dist), then each chosen
+//     free node is pushed to X + normalize(X - c) t
+__device__ __forceinline__ float hash1(float v) { const float x = sinf(v * 91.3458f) * 47453.5453f; return x - floorf(x); }
+__device__ __forceinline__ float hash2(float a, float b) {
+    const float x = sinf(a * 12.9898f + b * 78.233f) * 43758.5453f;
+    return x - floorf(x);
+}
+
+__global__ void k_effect_nodes(const SceneDev* __restrict__ scene, const NWork* __restrict__ work, int slot) {
+    const NWork wk = work[blockIdx.x];
+    if (threadIdx.x >= wk.count) return;
+    const SceneDev& S = *scene;
+    const EffectDev& E = S.effects[slot];
+    if (!E.active) return;
+    const int i = wk.begin + threadIdx.x;
+    if (S.mask[i] == 0) return;
+    const float4 X = S.X[i];
+    float px, py, pz;
+    if (E.kind == 0) {
+        const float4 u = S.u[i];
+        px = X.x + u.x; py = 0.f; pz = X.z + u.z;
+    } else {
+        const float h = hash1(X.z);   // vec3_to_scalar_random(init_p)
+        const float rx = hash2(X.x + h, X.y + h) * 2.f - 1.f;
+        const float ry = hash1(rx * (float)i) * 2.f - 1.f;
+        const float rz = hash1(rx * ry) * 2.f - 1.f;
+        const float r = hash1(rz * rx * ry);
+        const float inv = 1.f / sqrtf(rx * rx + ry * ry + rz * rz);
+        px = E.cx + rx * inv * E.radius * r; py = E.cy + ry * inv * E.radius * r; pz = E.cz + rz * inv * E.radius * r;
+    }
+    const float4 u = make_float4(px - X.x, py - X.y, pz - X.z, 0.f);
+    S.u[i] = u;
+    S.u_last[i] = u;
+    S.v[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+__global__ void k_effect_stretch(const SceneDev* __restrict__ scene, int slot, float dt) {
+    const SceneDev& S = *scene;
+    const EffectDev& E = S.effects[slot];
+    if (!E.active) return;
+    __shared__ float t;
+    if (threadIdx.x == 0) {
+        t = fminf(*E.t + dt, E.max_dist);
+        *E.t = t;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < E.n; k += blockDim.x) {
+        const int id = E.ids[k];
+        if (S.mask[id] == 0) continue;
+        const float4 X = S.X[id];
+        const float dx = X.x - E.cx, dy = X.y - E.cy, dz = X.z - E.cz;
+        const float inv = 1.f / sqrtf(dx * dx + dy * dy + dz * dz);
+        const float4 u = S.u[id];
+        S.u[id] = make_float4(dx * inv * t, dy * inv * t, dz * inv * t, u.w);
+    }
+}
+
 // Host-state staging of a batch: state[off_s + 3 i ...] = u_i then v_i (n*3 floats each).
 // dir 0: staging -> node arrays, dir 1: node arrays -> staging.
 __global__ void k_state(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work, const long long* __restrict__ soff,
@@ -1356,6 +1418,11 @@ void launch_velocity(const SceneDev* scenes, const NWork* work, int n_work, floa
 void launch_chebyshev(const SceneDev* scenes, const NWork* work, int n_work, const StepParams& P, cudaStream_t st) {
     if (n_work <= 0) return;
     k_chebyshev<<<n_work, kNodeChunk, 0, st>>>(scenes, work, n_work, P);
+}
+
+void launch_effect(const SceneDev* scene, const NWork* work, int n_work, int slot, int kind, float dt, cudaStream_t st) {
+    if (kind == 2) k_effect_stretch<<<1, 256, 0, st>>>(scene, slot, dt);
+    else if (n_work > 0) k_effect_nodes<<<n_work, kNodeChunk, 0, st>>>(scene, work, slot);
 }
 
 void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, int box_pass, cudaStream_t st) {

@@ -23,6 +23,9 @@ void launch_velocity(const SceneDev* scenes, const NWork* work, int n_work, floa
 void launch_chebyshev(const SceneDev* scenes, const NWork* work, int n_work, const StepParams& P, cudaStream_t st);
 // box_pass 0: work indexes fixed-id chunks; 1: work indexes node chunks (box clamp)
 void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, int box_pass, cudaStream_t st);
+// One scripted effect of one scene (kind 0 crush / 1 random sphere over the node chunks in
+// work, kind 2 high stretch over its ids); a no-op while the effect is inactive.
+void launch_effect(const SceneDev* scene, const NWork* work, int n_work, int slot, int kind, float dt, cudaStream_t st);
 // raw: the kernel_XPBD_V1/V2 update form (ignored for Tetra4, which always uses V0)
 void launch_xpbd(int element, int material, bool raw, const SceneDev* scenes, const int* elems, int begin, int count,
                  int scene, const StepParams& P, cudaStream_t st);

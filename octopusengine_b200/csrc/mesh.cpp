@@ -10,7 +10,10 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <map>
+#include <set>
 #include <unordered_map>
+#include <vector>
 
 #include "host.hpp"
 
@@ -228,6 +231,46 @@ void lumped_masses(int e, const float* X, int n, const int32_t* T, int n_elem, f
         total /= (float)n;
         for (int i = 0; i < n; ++i) mass[i] = total;
     }
+}
+
+// Nodes on the mesh boundary, ascending (MeshTools::Get_Surface_Geometry_Ids,
+// octopus/include/Mesh/MeshTools.h:64-89: the nodes of the element faces that no other element
+// shares).  A face is keyed by its sorted corner ids; its nodes are every node of the element
+// whose reference coordinates lie on that face (corners, edge and face nodes).
+std::vector<int32_t> surface_nodes(int e, const int32_t* T, int n_elem) {
+    const int ne = element_nodes(e);
+    std::vector<double> rn(3 * ne);
+    reference_nodes(e, rn.data());
+    const bool tet = e == kTetra || e == kTetra10 || e == kTetra20;
+    const int nc = tet ? 4 : 8, nf = tet ? 4 : 6;
+    // on_face[f] = local nodes on face f
+    std::vector<std::vector<int>> on_face(nf);
+    for (int j = 0; j < ne; ++j) {
+        const double* x = &rn[3 * j];
+        for (int f = 0; f < nf; ++f) {
+            bool on;
+            if (tet) on = std::fabs(f == 0 ? 1.0 - x[0] - x[1] - x[2] : x[f - 1]) < 1e-9;   // L_f = 0
+            else on = std::fabs(x[f / 2] - (f % 2 ? 1.0 : -1.0)) < 1e-9;
+            if (on) on_face[f].push_back(j);
+        }
+    }
+    std::map<std::vector<int32_t>, std::pair<int, std::pair<int, int>>> faces;   // corners -> (count, (element, face))
+    for (int el = 0; el < n_elem; ++el)
+        for (int f = 0; f < nf; ++f) {
+            std::vector<int32_t> key;
+            for (int j : on_face[f]) if (j < nc) key.push_back(T[(size_t)el * ne + j]);
+            std::sort(key.begin(), key.end());
+            auto it = faces.find(key);
+            if (it == faces.end()) faces.emplace(key, std::make_pair(1, std::make_pair(el, f)));
+            else it->second.first++;
+        }
+    std::set<int32_t> ids;
+    for (const auto& [key, v] : faces) {
+        if (v.first != 1) continue;
+        const int el = v.second.first, f = v.second.second;
+        for (int j : on_face[f]) ids.insert(T[(size_t)el * ne + j]);
+    }
+    return std::vector<int32_t>(ids.begin(), ids.end());
 }
 
 }  // namespace octb

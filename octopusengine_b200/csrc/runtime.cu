@@ -124,6 +124,11 @@ struct oct_scene {
     std::vector<int> elem_off;
     double* d_red = nullptr;        // 4 doubles of reduction scratch
     float* d_diag = nullptr;        // per-element diagnostics output (allocated on first use)
+    // scripted effects (oct_scene_add_effect): host copy of the device slots
+    EffectDev effects[kMaxEffects];
+    EffectDev* d_effects = nullptr;
+    int n_effects = 0;
+    std::vector<int32_t> topo_host;   // kept for the effects' surface extraction
 };
 
 struct oct_batch {
@@ -527,6 +532,10 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
         if ((st = upload(c, s->mem, entd, ent))) return st;
         h.ent = entd;
     }
+    for (int k = 0; k < kMaxEffects; ++k) { s->effects[k] = EffectDev{}; s->effects[k].kind = -1; }
+    if ((st = upload(c, s->mem, s->d_effects, std::vector<EffectDev>(s->effects, s->effects + kMaxEffects)))) return st;
+    h.effects = s->d_effects;
+    s->topo_host.assign(d->topology, d->topology + (size_t)E * NE);
     if ((st = s->mem.alloc(s->d_scene, 1))) return st;
     OCT_CUDA(c, cudaMemcpy(s->d_scene, &h, sizeof(SceneDev), cudaMemcpyHostToDevice));
     s->pending_host = s->has_v0 ? 1 : 0;
@@ -551,6 +560,14 @@ StepParams base_params(oct_ctx* c, float dt) {
     P.omega = 1.f;
     P.error = c->d_error;
     return P;
+}
+
+// Scripted effects of one scene, in creation order (each a no-op while inactive).
+void enqueue_effects(oct_scene* s, float dt, cudaStream_t st) {
+    for (int k = 0; k < s->n_effects; ++k) {
+        launch_effect(s->d_scene, s->d_nwork, s->n_nwork, k, s->effects[k].kind, dt, st);
+        s->ctx->launches++;
+    }
 }
 
 // One GPU_VBD::step (octopus/src/GPU/VBD/GPU_VBD.cu:38-61) of one scene with the reference's
@@ -581,6 +598,7 @@ void vbd_substep(oct_scene* s, float dt) {
             if (!s->in_place) { launch_commit(s->d_scene, s->d_vwork + b, n, st); c->launches++; }
         }
         if (s->n_fixed) { launch_constraints(s->d_scene, s->d_fwork, s->n_fwork, 0, st); c->launches++; }
+        enqueue_effects(s, dt, st);
         if (s->box) { launch_constraints(s->d_scene, s->d_nwork, s->n_nwork, 1, st); c->launches++; }
         if (cheb) {
             if (j == 1) omega = 2.f / (2.f - s->rho * s->rho);
@@ -608,6 +626,7 @@ void xpbd_substep(oct_scene* s, float dt) {
         c->launches++;
     }
     if (s->n_fixed) { launch_constraints(s->d_scene, s->d_fwork, s->n_fwork, 0, st); c->launches++; }
+    enqueue_effects(s, dt, st);
     if (s->box) { launch_constraints(s->d_scene, s->d_nwork, s->n_nwork, 1, st); c->launches++; }
     launch_velocity(s->d_scene, s->d_nwork, s->n_nwork, s->global_damping, 1, P, st);
     c->launches++;
@@ -622,6 +641,7 @@ void explicit_substep(oct_scene* s, float dt) {
     launch_predict(s->d_scene, s->d_nwork, s->n_nwork, 1, 1, 0, P, st);
     c->launches += 2;
     if (s->n_fixed) { launch_constraints(s->d_scene, s->d_fwork, s->n_fwork, 0, st); c->launches++; }
+    enqueue_effects(s, dt, st);
     if (s->box) { launch_constraints(s->d_scene, s->d_nwork, s->n_nwork, 1, st); c->launches++; }
 }
 
@@ -909,6 +929,90 @@ oct_status oct_scene_set_fixation(oct_scene* s, const float offset[3], const flo
     return oct_scene_set_fixation_group(s, 0, offset, rotation);
 }
 
+oct_status oct_scene_add_effect(oct_scene* s, int kind, const float* params, int32_t* index) {
+    if (!s || kind < OCT_EFFECT_CRUSH || kind > OCT_EFFECT_HIGH_STRETCH) return OCT_EINVAL;
+    if (s->n_effects >= kMaxEffects) return fail(s->ctx, OCT_ENOTSUP, "at most 4 effects per scene");
+    oct_ctx* c = s->ctx;
+    EffectDev e{};
+    e.kind = kind;
+    e.active = 0;   // created inactive, as the reference controller creates them
+    // centre: sum of the rest positions after the first, divided by their count (the
+    // GPU_RandomSphere / GPU_HighStretch constructors, GPU_Constraint.h:29-31,44-45)
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    for (int i = 1; i < s->n_nodes; ++i) { cx += s->X[3 * i]; cy += s->X[3 * i + 1]; cz += s->X[3 * i + 2]; }
+    const float inv = 1.f / (float)s->n_nodes;
+    e.cx = cx * inv; e.cy = cy * inv; e.cz = cz * inv;
+    if (kind == OCT_EFFECT_RANDOM_SPHERE) {
+        if (!params || !(params[0] > 0.f)) return OCT_EINVAL;
+        e.radius = params[0];
+    } else if (kind == OCT_EFFECT_HIGH_STRETCH) {
+        if (!params || params[0] < 1.f || params[0] > 1024.f || !(params[1] >= 0.f)) return OCT_EINVAL;
+        const int nb = (int)params[0];
+        e.max_dist = params[1];
+        // farthest-point choice among the boundary nodes (GPU_HighStretch ctor, :41-66): start
+        // at the lowest surface id, then repeatedly the node farthest from the chosen ones
+        const std::vector<int32_t> ids = surface_nodes(s->element, s->topo_host.data(), s->n_elements);
+        std::vector<int32_t> chosen;
+        std::vector<char> taken(s->n_nodes, 0);
+        for (int i = 0; i < nb && !ids.empty(); ++i) {
+            float best = 0.f;
+            int cur = ids[0];
+            for (int32_t a : ids) {
+                if (taken[a]) continue;
+                float d = 3.402823466e38f;
+                for (int32_t b : chosen) {
+                    const float dx = s->X[3 * a] - s->X[3 * b], dy = s->X[3 * a + 1] - s->X[3 * b + 1],
+                                dz = s->X[3 * a + 2] - s->X[3 * b + 2];
+                    d = std::min(d, dx * dx + dy * dy + dz * dz);
+                }
+                if (d > best) { cur = a; best = d; }
+            }
+            chosen.push_back(cur);
+            taken[cur] = 1;
+        }
+        oct_status st;
+        int32_t* d_ids = nullptr;
+        float* d_t = nullptr;
+        if ((st = upload(c, s->mem, d_ids, chosen)) || (st = upload(c, s->mem, d_t, std::vector<float>{0.f}))) return st;
+        e.ids = d_ids;
+        e.n = (int)chosen.size();
+        e.t = d_t;
+    }
+    const int k = s->n_effects;
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    OCT_CUDA(c, cudaMemcpy(s->d_effects + k, &e, sizeof(EffectDev), cudaMemcpyHostToDevice));
+    s->effects[k] = e;
+    s->n_effects++;
+    drop_frame_graph(s);
+    if (index) *index = k;
+    return OCT_OK;
+}
+
+oct_status oct_scene_set_effect_active(oct_scene* s, int32_t index, int active) {
+    if (!s || index < 0 || index >= s->n_effects) return OCT_EINVAL;
+    s->effects[index].active = active ? 1 : 0;
+    OCT_CUDA(s->ctx, cudaMemcpyAsync(&s->d_effects[index].active, &s->effects[index].active, sizeof(int),
+                                     cudaMemcpyHostToDevice, s->ctx->stream));
+    OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    return OCT_OK;
+}
+
+oct_status oct_scene_effect_ids(oct_scene* s, int32_t index, int32_t* ids, int32_t* n) {
+    if (!s || !n || index < 0 || index >= s->n_effects) return OCT_EINVAL;
+    const EffectDev& e = s->effects[index];
+    *n = e.kind == OCT_EFFECT_HIGH_STRETCH ? e.n : 0;
+    if (ids && *n) OCT_CUDA(s->ctx, cudaMemcpy(ids, e.ids, sizeof(int32_t) * e.n, cudaMemcpyDeviceToHost));
+    return OCT_OK;
+}
+
+oct_status oct_surface_nodes(int32_t element, const int32_t* topology, int32_t n_elements, int32_t* ids, int32_t* n) {
+    if (!topology || n_elements <= 0 || !n || element_nodes(element) < 0) return OCT_EINVAL;
+    const std::vector<int32_t> v = surface_nodes(element, topology, n_elements);
+    *n = (int32_t)v.size();
+    if (ids) std::copy(v.begin(), v.end(), ids);
+    return OCT_OK;
+}
+
 oct_status oct_scene_set_precision(oct_scene* s, int precision) {
     if (!s || precision < 0 || precision > 1) return OCT_EINVAL;
     s->precision = precision;
@@ -1108,6 +1212,8 @@ void batch_substep(oct_batch* b, float dt) {
             cudaStreamWaitEvent(st, g.done, 0);
         }
         if (b->n_fwork) launch_constraints(b->d_scenes, b->d_fwork, b->n_fwork, 0, st);
+        for (auto* s : b->scenes)
+            for (int k = 0; k < s->n_effects; ++k) launch_effect(s->d_scene, s->d_nwork, s->n_nwork, k, s->effects[k].kind, dt, st);
         if (b->n_bwork) launch_constraints(b->d_scenes, b->d_bwork, b->n_bwork, 1, st);
         if (cheb) {
             if (j == 1) omega = 2.f / (2.f - b->rho * b->rho);

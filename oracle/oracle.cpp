@@ -649,6 +649,9 @@ template <class T> struct State {
     M3<T> R[4];
     bool box = false;
     V3<T> bmin, bmax;
+    // scripted effects (GPU_Crush / GPU_RandomSphere / GPU_HighStretch)
+    struct Effect { int kind; bool active; std::vector<int> ids; V3<T> c; T radius, max_dist, t; };
+    std::vector<Effect> effects;
 };
 
 // GPU_ParticleSystem ctor (GPU_ParticleSystem.cu:6-22) and GPU_Fix_Constraint ctor
@@ -694,13 +697,50 @@ template <class T> void init_state(const orc_desc* d, State<T>& s) {
 
 // kernel_constraint_fix (GPU_Constraint.cu:8-20) with identity rotation and zero offset,
 // then kernel_constraint_box_limit (:80-92) when enabled.
-template <class T> void apply_constraints(State<T>& s) {
+// The sine hash of kernel_constraint_random_sphere (GPU_Constraint.cu:36-51), in T.
+template <class T> T fract(T x) { return x - std::floor(x); }
+template <class T> T hash1(T v) { return fract(std::sin(v * T(91.3458f)) * T(47453.5453f)); }
+template <class T> T hash2(T a, T b) { return fract(std::sin(a * T(12.9898f) + b * T(78.233f)) * T(43758.5453f)); }
+
+template <class T> void apply_constraints(State<T>& s, T dt) {
     for (size_t k = 0; k < s.fixed.size(); ++k) {
         const int id = s.fixed[k], g = s.fgroup[k];
         s.p[id] = s.off[g] + s.com[g] + s.R[g] * (s.init_p[id] - s.com[g]);
         s.v[id] = V3<T>();
         s.f[id] = V3<T>();
         s.mask[id] = 0;
+    }
+    // effects after the fixation, in creation order (kernel_constraint_crush / random_sphere /
+    // high_stretch, GPU_Constraint.cu:22-92)
+    for (auto& e : s.effects) {
+        if (!e.active) continue;
+        if (e.kind == 2) {
+            e.t = std::min(e.t + dt, e.max_dist);
+            for (int id : e.ids) {
+                if (s.mask[id] == 0) continue;
+                const V3<T> d = s.init_p[id] - e.c;
+                s.p[id] = s.init_p[id] + d / length(d) * e.t;
+            }
+            continue;
+        }
+        for (int i = 0; i < s.n; ++i) {
+            if (s.mask[i] == 0) continue;
+            if (e.kind == 0) {
+                s.p[i].y = T(0);
+            } else {
+                const V3<T>& x = s.init_p[i];
+                const T h = hash1(x.z);
+                const T rx = hash2(x.x + h, x.y + h) * T(2) - T(1);
+                const T ry = hash1(rx * T(i)) * T(2) - T(1);
+                const T rz = hash1(rx * ry) * T(2) - T(1);
+                const T r = hash1(rz * rx * ry);
+                const V3<T> d(rx, ry, rz);
+                s.p[i] = e.c + d / length(d) * (e.radius * r);
+            }
+            s.last_p[i] = s.p[i];
+            s.v[i] = V3<T>();
+            s.f[i] = V3<T>();
+        }
     }
     if (s.box)
         for (int i = 0; i < s.n; ++i) {
@@ -813,7 +853,7 @@ template <class T> void vbd_substep(VBD<T>& b, T dt) {
                 for (int vid : vs) if (s.mask[vid] != 0) s.p[vid] = s.p_new[vid];   // kernel_copy_in_position
             }
         }
-        apply_constraints(s);
+        apply_constraints(s, dt);
         if (b.rho > T(0) && b.rho > T(1.17549435e-38f * 1e6f)) {   // GPU_VBD.cu:50-56
             if (j == 1) omega = T(2) / (T(2) - b.rho * b.rho);
             else if (j > 1) omega = T(4) / (T(4) - b.rho * b.rho * omega);
@@ -1169,7 +1209,7 @@ template <class T> void xpbd_substep(XPBD<T>& x, T dt) {
                 }
             }
         }
-    apply_constraints(s);
+    apply_constraints(s, dt);
     for (int i = 0; i < s.n; ++i) {
         s.v[i] = (s.p[i] - s.last_p[i]) / dt;
         const T nv = length(s.v[i]);
@@ -1221,7 +1261,7 @@ template <class T> void explicit_substep(Explicit<T>& x, T dt) {
         s.p[i] = s.p[i] + s.v[i] * dt;
         s.f[i] = V3<T>();
     }
-    apply_constraints(s);
+    apply_constraints(s, dt);
 }
 
 template <class T> int get_state(const State<T>& s, int what, double* out) {
@@ -1275,6 +1315,30 @@ template <class T> Explicit<T>* explicit_create_t(const orc_desc* d) {
 template <class T> void set_fix(State<T>& s, int g, const float* off, const float* rot) {
     if (off) s.off[g] = {(T)off[0], (T)off[1], (T)off[2]};
     if (rot) for (int j = 0; j < 3; ++j) s.R[g][j] = {(T)rot[3 * j], (T)rot[3 * j + 1], (T)rot[3 * j + 2]};
+}
+
+template <class T> int add_effect(State<T>& s, int kind, const float* params, const int32_t* ids, int n_ids) {
+    typename State<T>::Effect e{};
+    e.kind = kind;
+    e.active = false;
+    // centre: (sum of the positions after the first) / count, in FP32 as the constructors
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    for (int i = 1; i < s.n; ++i) { cx += (float)s.init_p[i].x; cy += (float)s.init_p[i].y; cz += (float)s.init_p[i].z; }
+    const float inv = 1.f / (float)s.n;
+    e.c = {(T)(cx * inv), (T)(cy * inv), (T)(cz * inv)};
+    e.radius = kind == 1 ? (T)params[0] : T(0);
+    e.max_dist = kind == 2 ? (T)params[1] : T(0);
+    e.t = T(0);
+    if (kind == 2) e.ids.assign(ids, ids + n_ids);
+    s.effects.push_back(e);
+    return (int)s.effects.size() - 1;
+}
+template <class T> State<T>* state_of(Handle* h) {
+    switch (h->kind) {
+        case 0: case 1: return &((VBD<T>*)h->ptr)->s;
+        case 2: case 3: return &((XPBD<T>*)h->ptr)->s;
+        default: return &((Explicit<T>*)h->ptr)->s;
+    }
 }
 
 }  // namespace orc
@@ -1452,6 +1516,28 @@ int orc_vbd_step(void* hv, float frame_dt, int substeps) {
     for (int k = 0; k < substeps; ++k) {
         if (h->kind == 1) vbd_substep(*(VBD<double>*)h->ptr, (double)sub);
         else vbd_substep(*(VBD<float>*)h->ptr, sub);
+    }
+    return 0;
+}
+
+int orc_add_effect(void* hv, int kind, const float* params, const int32_t* ids, int n_ids) {
+    Handle* h = (Handle*)hv;
+    if (!h || kind < 0 || kind > 2 || (kind > 0 && !params) || (kind == 2 && n_ids > 0 && !ids)) return -1;
+    const bool fp64 = h->kind % 2 == 1;
+    return fp64 ? add_effect(*state_of<double>(h), kind, params, ids, n_ids) : add_effect(*state_of<float>(h), kind, params, ids, n_ids);
+}
+
+int orc_set_effect_active(void* hv, int index, int active) {
+    Handle* h = (Handle*)hv;
+    if (!h) return -1;
+    if (h->kind % 2 == 1) {
+        auto& v = state_of<double>(h)->effects;
+        if (index < 0 || index >= (int)v.size()) return -1;
+        v[index].active = active != 0;
+    } else {
+        auto& v = state_of<float>(h)->effects;
+        if (index < 0 || index >= (int)v.size()) return -1;
+        v[index].active = active != 0;
     }
     return 0;
 }

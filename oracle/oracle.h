@@ -91,6 +91,12 @@ int orc_element_data(void* h, int kind, double* out);
  * R column-major; works on VBD, XPBD and explicit handles. */
 int orc_set_fixation(void* h, int group, const float* offset, const float* rotation);
 
+/* Scripted effect on any handle (GPU_Crush kind 0, GPU_RandomSphere kind 1 with params[0] the
+ * radius, GPU_HighStretch kind 2 with params[1] the maximum distance and the moved ids), created
+ * inactive; returns its index.  Effects run after the fixation, in creation order. */
+int orc_add_effect(void* h, int kind, const float* params, const int32_t* ids, int n_ids);
+int orc_set_effect_active(void* h, int index, int active);
+
 /* Polar decomposition F = R S of mat3x3_polardecomposition (CUMatrix.cu:75-96), column-major,
  * in float (fp64 = 0) or double; and one XPBD constraint pair (eval_material,
  * GPU_PBD_FEM_Materials.cu:97-117) in double. */

@@ -67,6 +67,8 @@ def lib():
         L.orc_cpuvbd_run_many.restype = C.c_double
         L.orc_polar.argtypes = [dp, C.c_int, dp, dp]
         L.orc_element_data.argtypes = [vp, C.c_int, dp]
+        L.orc_add_effect.argtypes = [vp, C.c_int, fp, ip, C.c_int]
+        L.orc_set_effect_active.argtypes = [vp, C.c_int, C.c_int]
         L.orc_vbd_forces.argtypes = [vp, C.c_float, dp]
         L.orc_xpbd_pair.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, dp, dp, dp]
         _lib = L
@@ -229,6 +231,16 @@ class Solver:
         e = np.zeros(4)
         lib().orc_vbd_energy(self.h, _p(e, C.c_double))
         return e
+
+    def add_effect(self, kind, params=(0.0, 0.0), ids=()):
+        p = np.asarray(list(params) + [0.0] * 2, np.float32)
+        i = np.ascontiguousarray(ids, np.int32)
+        k = lib().orc_add_effect(self.h, kind, _p(p, C.c_float), _p(i, C.c_int32) if len(i) else None, len(i))
+        assert k >= 0
+        return k
+
+    def set_effect_active(self, index, active=True):
+        assert lib().orc_set_effect_active(self.h, index, int(active)) == 0
 
     def set(self, what, values):
         """VBD state write (what: 0 p, 1 v, 2 last_p, 3 y)."""
