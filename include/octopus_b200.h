@@ -169,6 +169,8 @@ oct_status oct_scene_set_precision(oct_scene* s, int precision);
  *                             node centroid by the reference's sine hash
  *   OCT_EFFECT_HIGH_STRETCH   params[0] boundary nodes chosen farthest-first are pushed away
  *                             from the centroid by t, t growing by dt per call up to params[1]
+ * Deactivating a high stretch resets its distance to 0, as the controller does when it turns the
+ * effect off (Cuda_Constraint_Rigid_Controller.cpp:72-76,150-153).
  * Effects are created inactive (as the controller creates them) and run, while active, after
  * the fixation and before the box limit, in creation order, wherever the constraints run (every
  * VBD iteration; every XPBD or explicit sub-step).  At most 4 per scene; add them before the

@@ -16,6 +16,7 @@
 // being ignored; the colour order is ascending (reproducible) instead of clock-shuffled;
 // no VTK side file is written on construction.
 #pragma once
+#include <cstring>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -156,7 +157,21 @@ struct GPU_FEM_Explicit : GPU_FEM {
         : GPU_FEM(e, g, t, young_, poisson_, m) { damping = damping_; }
 };
 
-// GPU_Fix_Constraint(positions, Area*) (octopus/src/GPU/GPU_Constraint.cu:94-107).
+// Axis (octopus/include/Tools/Axis.h): a position and a rotation (column-major 3x3).
+struct Axis {
+    Vector3 pos{0.f, 0.f, 0.f};
+    float rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    void move(const Vector3& m) { pos = Vector3(pos.x + m.x, pos.y + m.y, pos.z + m.z); }
+    void setPosition(const Vector3& p) { pos = p; }
+    void setRotation(const float r[9]) { for (int k = 0; k < 9; ++k) rot[k] = r[k]; }
+    const Vector3& position() const { return pos; }
+    const float* rotation() const { return rot; }
+};
+
+// GPU_Fix_Constraint(positions, Area*) (octopus/src/GPU/GPU_Constraint.cu:94-107): the nodes
+// inside the area follow com + axis.position + axis.rotation (X - com).  Each constraint of an
+// integrator is one rigid group of the scene (at most four); moving its axis between steps
+// moves the group.
 struct GPU_Fix_Constraint : GPU_Dynamic {
     GPU_Fix_Constraint(const Mesh::Geometry& positions, Area* area) {
         if (auto* p = dynamic_cast<Plane*>(area)) {
@@ -169,6 +184,36 @@ struct GPU_Fix_Constraint : GPU_Dynamic {
         delete area;
     }
     std::vector<int> ids;
+    Axis axis;
+    float sent[12] = {0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1};   // axis last sent to the scene (the identity at set-up)
+};
+
+// GPU_Box_Limit(pmin, pmax) (octopus/include/GPU/GPU_Constraint.h:20-25): free nodes clamped
+// to the box (one box per integrator).
+struct GPU_Box_Limit : GPU_Dynamic {
+    GPU_Box_Limit(const Vector3& pmin_, const Vector3& pmax_) : pmin(pmin_), pmax(pmax_) {}
+    Vector3 pmin, pmax;
+};
+
+// Scripted effects (octopus/include/GPU/GPU_Constraint.h:28-80); `active` is read at every step.
+struct GPU_Effect : GPU_Dynamic {
+    int kind = OCT_EFFECT_CRUSH;
+    float params[2] = {0.f, 0.f};
+    int index = -1;         // slot in the scene, set at the first step
+    bool applied = false;   // last active state sent to the scene
+};
+struct GPU_Crush : GPU_Effect {
+    GPU_Crush() { kind = OCT_EFFECT_CRUSH; }
+};
+struct GPU_RandomSphere : GPU_Effect {
+    GPU_RandomSphere(const Mesh::Geometry&, scalar radius) { kind = OCT_EFFECT_RANDOM_SPHERE; params[0] = radius; }
+};
+struct GPU_HighStretch : GPU_Effect {
+    GPU_HighStretch(int nb_constraint, scalar max_dist) {
+        kind = OCT_EFFECT_HIGH_STRETCH;
+        params[0] = (float)nb_constraint;
+        params[1] = max_dist;
+    }
 };
 
 // GPU_Integrator and the three solvers (octopus/include/GPU/GPU_Integrator.h:11-36).
@@ -177,6 +222,24 @@ struct GPU_Integrator : GPU_Dynamic {
     virtual void add_constraint(GPU_Dynamic* c) { constraints.push_back(c); }
     void step(GPU_ParticleSystem* ps, scalar dt) override {
         if (!ps->scene) commit(ps);
+        // constraint state read at every step: fixation axes and effect activity
+        int g = 0;
+        for (auto* c : constraints) {
+            if (auto* f = dynamic_cast<GPU_Fix_Constraint*>(c)) {
+                const float off[3] = {f->axis.pos.x, f->axis.pos.y, f->axis.pos.z};
+                if (std::memcmp(off, f->sent, sizeof(off)) != 0 || std::memcmp(f->axis.rot, f->sent + 3, sizeof(f->axis.rot)) != 0) {
+                    check(oct_scene_set_fixation_group(ps->scene, g, off, f->axis.rot), "fixation axis");
+                    std::memcpy(f->sent, off, sizeof(off));
+                    std::memcpy(f->sent + 3, f->axis.rot, sizeof(f->axis.rot));
+                }
+                ++g;
+            } else if (auto* e = dynamic_cast<GPU_Effect*>(c)) {
+                if (e->active != e->applied) {
+                    check(oct_scene_set_effect_active(ps->scene, e->index, e->active ? 1 : 0), "effect");
+                    e->applied = e->active;
+                }
+            }
+        }
         check(oct_scene_step(ps->scene, dt, 1), "GPU_Integrator::step", default_context());
     }
     ~GPU_Integrator() override {
@@ -199,9 +262,14 @@ struct GPU_Integrator : GPU_Dynamic {
         for (size_t i = 0; i < ps->init_positions.size(); ++i) {
             X[3 * i] = ps->init_positions[i].x; X[3 * i + 1] = ps->init_positions[i].y; X[3 * i + 2] = ps->init_positions[i].z;
         }
-        std::vector<int> fixed;
+        std::vector<int> fixed, group;
+        int n_groups = 0;
         for (auto* c : constraints)
-            if (auto* f = dynamic_cast<GPU_Fix_Constraint*>(c)) fixed.insert(fixed.end(), f->ids.begin(), f->ids.end());
+            if (auto* f = dynamic_cast<GPU_Fix_Constraint*>(c)) {
+                if (n_groups == 4) throw Error(OCT_ENOTSUP, "at most four GPU_Fix_Constraint per integrator");
+                fixed.insert(fixed.end(), f->ids.begin(), f->ids.end());
+                group.insert(group.end(), f->ids.size(), n_groups++);
+            }
         const int ne = fem->element == Tetra ? 4 : fem->element == Hexa ? 8 : fem->element == Tetra10 ? 10 :
                        fem->element == Tetra20 ? 20 : 27;
         d.element = fem->element;
@@ -217,12 +285,21 @@ struct GPU_Integrator : GPU_Dynamic {
         for (int k = 0; k < 3; ++k) d.gravity[k] = gravity[k];
         d.n_fixed = (int)fixed.size();
         d.fixed_ids = fixed.empty() ? nullptr : fixed.data();
+        d.fixed_group = fixed.empty() ? nullptr : group.data();
+        for (auto* c : constraints)
+            if (auto* b = dynamic_cast<GPU_Box_Limit*>(c)) {
+                d.box_limit = 1;
+                d.box_min[0] = b->pmin.x; d.box_min[1] = b->pmin.y; d.box_min[2] = b->pmin.z;
+                d.box_max[0] = b->pmax.x; d.box_max[1] = b->pmax.y; d.box_max[2] = b->pmax.z;
+            }
         fill(d);
         if (auto* v = dynamic_cast<GPU_VBD_FEM*>(fem)) { d.vbd_version = v->version; d.target_color = v->target_color; }
         if (auto* x = dynamic_cast<GPU_PBD_FEM*>(fem)) d.xpbd_version = x->version;
         oct_ctx* ctx = default_context();
         check(oct_scene_create(ctx, &d, &owned), "oct_scene_create", ctx);
         ps->scene = owned;
+        for (auto* c : constraints)
+            if (auto* e = dynamic_cast<GPU_Effect*>(c)) check(oct_scene_add_effect(owned, e->kind, e->params, &e->index), "effect", ctx);
     }
     oct_scene* owned = nullptr;
 };

@@ -993,6 +993,8 @@ oct_status oct_scene_set_effect_active(oct_scene* s, int32_t index, int active) 
     s->effects[index].active = active ? 1 : 0;
     OCT_CUDA(s->ctx, cudaMemcpyAsync(&s->d_effects[index].active, &s->effects[index].active, sizeof(int),
                                      cudaMemcpyHostToDevice, s->ctx->stream));
+    if (!active && s->effects[index].kind == OCT_EFFECT_HIGH_STRETCH)   // the controller restarts the stretch
+        OCT_CUDA(s->ctx, cudaMemsetAsync(s->effects[index].t, 0, sizeof(float), s->ctx->stream));
     OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
     return OCT_OK;
 }
