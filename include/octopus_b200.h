@@ -110,6 +110,13 @@ typedef struct oct_scene_desc {
                                        (vertex, owner) pair packed into warps, 1..32 = lanes per
                                        vertex (power of two) */
     int32_t xpbd_version;           /* OCT_XPBD_* (default OCT_XPBD_OPTISHARED) */
+    float mg_linear;                /* multigrid VBD for P2 / Q2 (MG_VBD_FEM,
+                                       octopus/include/Dynamic/VBD/MG_VertexBlockDescent.h:52-74):
+                                       fraction of the iterations solved on the linear mesh of
+                                       the corners, with its own colouring and masses (from
+                                       density and mass_distribution); mid nodes follow by
+                                       prolongation.  0 = off.  Such scenes are stepped alone
+                                       (no batch, no frame graph), without Chebyshev. */
 } oct_scene_desc;
 
 /* Context: device, stream, HBM budget (bytes; 0 = 90% of free device memory). */

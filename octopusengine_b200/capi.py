@@ -82,7 +82,7 @@ class SceneDesc(C.Structure):
         ("rho", C.c_float), ("vbd_version", C.c_int32), ("target_color", C.c_int32), ("color_algo", C.c_int32),
         ("order_mode", C.c_int32), ("seed", C.c_uint64), ("global_damping", C.c_float), ("precision", C.c_int32),
         ("box_limit", C.c_int32), ("box_min", C.c_float * 3), ("box_max", C.c_float * 3),
-        ("threads_per_vertex", C.c_int32), ("xpbd_version", C.c_int32),
+        ("threads_per_vertex", C.c_int32), ("xpbd_version", C.c_int32), ("mg_linear", C.c_float),
     ]
 
 

@@ -754,6 +754,42 @@ __global__ void k_effect_stretch(const SceneDev* __restrict__ scene, int slot, f
     }
 }
 
+// Multigrid VBD (MG_VBD_FEM, MG_VertexBlockDescent.cpp): the linear level is a scene of the
+// corner nodes.  gather copies the corners' displacement, start-of-sub-step displacement,
+// inertial target (its own masses kept) and mask into it; scatter copies the solved corners
+// back; prolong moves each mid node by the mean displacement since the sub-step start of its
+// k corners (P1_to_P2 / Q1_to_Q2::prolongation, :37-96).  list: per entry the mid node then
+// its k corners.
+__global__ void k_mg_copy(const SceneDev* __restrict__ main, const SceneDev* __restrict__ sub, const int* __restrict__ map,
+                          int n, int dir) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int m = map[k];
+    if (dir == 0) {
+        sub->u[k] = main->u[m];
+        sub->u_last[k] = main->u_last[m];
+        const float4 y = main->y[m];
+        const float w = sub->y[k].w;
+        sub->y[k] = make_float4(y.x, y.y, y.z, w);
+        sub->mask[k] = main->mask[m];
+    } else {
+        main->u[m] = sub->u[k];
+    }
+}
+
+__global__ void k_mg_prolong(const SceneDev* __restrict__ main, const int* __restrict__ list, int count, int k, float w) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int* e = list + (size_t)i * (k + 1);
+    float dx = 0.f, dy = 0.f, dz = 0.f;
+    for (int j = 1; j <= k; ++j) {
+        const float4 u = main->u[e[j]], ul = main->u_last[e[j]];
+        dx += u.x - ul.x; dy += u.y - ul.y; dz += u.z - ul.z;
+    }
+    const float4 ul = main->u_last[e[0]];
+    main->u[e[0]] = make_float4(ul.x + dx * w, ul.y + dy * w, ul.z + dz * w, ul.w);
+}
+
 // Host-state staging of a batch: state[off_s + 3 i ...] = u_i then v_i (n*3 floats each).
 // dir 0: staging -> node arrays, dir 1: node arrays -> staging.
 __global__ void k_state(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work, const long long* __restrict__ soff,
@@ -1423,6 +1459,13 @@ void launch_chebyshev(const SceneDev* scenes, const NWork* work, int n_work, con
 void launch_effect(const SceneDev* scene, const NWork* work, int n_work, int slot, int kind, float dt, cudaStream_t st) {
     if (kind == 2) k_effect_stretch<<<1, 256, 0, st>>>(scene, slot, dt);
     else if (n_work > 0) k_effect_nodes<<<n_work, kNodeChunk, 0, st>>>(scene, work, slot);
+}
+
+void launch_mg_copy(const SceneDev* main, const SceneDev* sub, const int* map, int n, int dir, cudaStream_t st) {
+    if (n > 0) k_mg_copy<<<(n + 255) / 256, 256, 0, st>>>(main, sub, map, n, dir);
+}
+void launch_mg_prolong(const SceneDev* main, const int* list, int count, int k, float w, cudaStream_t st) {
+    if (count > 0) k_mg_prolong<<<(count + 255) / 256, 256, 0, st>>>(main, list, count, k, w);
 }
 
 void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, int box_pass, cudaStream_t st) {

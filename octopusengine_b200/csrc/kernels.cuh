@@ -23,6 +23,10 @@ void launch_velocity(const SceneDev* scenes, const NWork* work, int n_work, floa
 void launch_chebyshev(const SceneDev* scenes, const NWork* work, int n_work, const StepParams& P, cudaStream_t st);
 // box_pass 0: work indexes fixed-id chunks; 1: work indexes node chunks (box clamp)
 void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, int box_pass, cudaStream_t st);
+// Multigrid VBD: corner copy between a scene and its linear level (dir 0 gather, 1 scatter)
+// and the prolongation of mid nodes from k corners with weight w.
+void launch_mg_copy(const SceneDev* main, const SceneDev* sub, const int* map, int n, int dir, cudaStream_t st);
+void launch_mg_prolong(const SceneDev* main, const int* list, int count, int k, float w, cudaStream_t st);
 // One scripted effect of one scene (kind 0 crush / 1 random sphere over the node chunks in
 // work, kind 2 high stretch over its ids); a no-op while the effect is inactive.
 void launch_effect(const SceneDev* scene, const NWork* work, int n_work, int slot, int kind, float dt, cudaStream_t st);

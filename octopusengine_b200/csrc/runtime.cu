@@ -129,6 +129,14 @@ struct oct_scene {
     EffectDev* d_effects = nullptr;
     int n_effects = 0;
     std::vector<int32_t> topo_host;   // kept for the effects' surface extraction
+    // multigrid VBD: the linear level as a scene of the corners, the corner map, the
+    // prolongation lists and the iteration schedule (MG_VBD_FEM)
+    oct_scene* mg_sub = nullptr;
+    int* d_mg_map = nullptr;
+    int n_mg_map = 0;
+    int* d_pro[3] = {nullptr, nullptr, nullptr};   // edges (k 2), faces (k 4), volumes (k 8)
+    int n_pro[3] = {0, 0, 0};
+    int mg_max[2] = {0, 0}, mg_count = 0, mg_current = 1;
 };
 
 struct oct_batch {
@@ -251,6 +259,85 @@ oct_status build_vertex_work(oct_scene* s) {
         s->vwork_off.push_back((int)vw.size());
     }
     return upload(s->ctx, s->mem, s->d_vwork, vw);
+}
+
+oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s);
+
+// Multigrid VBD (MG_VBD_FEM ctor, octopus/src/Dynamic/VBD/MG_VertexBlockDescent.cpp:134-176):
+// the linear level is built as a scene of the corner nodes (numbered in ascending order)
+// with the corner topology, its own DSAT colouring and lumped masses from the description's
+// density and distribution; max_it = {iterations - lin, lin}, lin = iterations x mg_linear.
+oct_status build_multigrid(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
+    if (d->solver != OCT_SOLVER_VBD || (d->element != kTetra10 && d->element != kHexa27))
+        return fail(c, OCT_ENOTSUP, "multigrid VBD needs a P2 or Q2 VBD scene");
+    if (d->rho > 0.f || d->order_mode != OCT_ORDER_ASCENDING)
+        return fail(c, OCT_ENOTSUP, "multigrid VBD runs without Chebyshev and in the ascending colour order");
+    if (!(d->mg_linear <= 1.f)) return fail(c, OCT_EINVAL, "mg_linear must be in (0, 1]");
+    const int N = d->n_nodes, E = d->n_elements, NE = s->ne, NL = d->element == kTetra10 ? 4 : 8;
+    std::vector<int32_t> compact(N, -1), back;
+    for (int e = 0; e < E; ++e) for (int j = 0; j < NL; ++j) compact[d->topology[(size_t)e * NE + j]] = 0;
+    for (int i = 0; i < N; ++i) if (compact[i] == 0) { compact[i] = (int32_t)back.size(); back.push_back(i); }
+    std::vector<int32_t> lt((size_t)E * NL);
+    for (int e = 0; e < E; ++e) for (int j = 0; j < NL; ++j) lt[(size_t)e * NL + j] = compact[d->topology[(size_t)e * NE + j]];
+    std::vector<float> lx(3 * back.size());
+    for (size_t k = 0; k < back.size(); ++k) for (int r = 0; r < 3; ++r) lx[3 * k + r] = d->positions[3 * back[k] + r];
+    oct_scene_desc dl = *d;
+    dl.element = d->element == kTetra10 ? kTetra : kHexa;
+    dl.n_nodes = (int32_t)back.size();
+    dl.positions = lx.data();
+    dl.topology = lt.data();
+    dl.masses = nullptr;
+    dl.n_fixed = 0; dl.fixed_ids = nullptr; dl.fixed_group = nullptr; dl.fix_by_plane = 0;
+    dl.initial_velocity = nullptr;
+    dl.box_limit = 0;
+    dl.threads_per_vertex = 0;
+    dl.mg_linear = 0.f;
+    auto* sub = new oct_scene();
+    oct_status st = build_scene(c, &dl, sub);
+    if (st) { sub->mem.release(); delete sub; return st; }
+    s->mg_sub = sub;
+    const int lin = (int)((float)s->iterations * d->mg_linear);
+    s->mg_max[0] = s->iterations - lin;
+    s->mg_max[1] = lin;
+    s->mg_count = 0;
+    s->mg_current = 1;
+    // prolongation lists, first visit in element order (P1_to_P2 / Q1_to_Q2 ctors, :13-34,
+    // :97-132); the reference's Q2 edge list ends with {7, 0} for node 19 (the edge is 7-4)
+    std::vector<int32_t> pro[3];
+    std::vector<char> seen(N, 0);
+    const int32_t* t = d->topology;
+    if (d->element == kTetra10) {
+        static const int ed[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+        for (int e = 0; e < E; ++e)
+            for (int j = 4; j < 10; ++j) {
+                const int v = t[(size_t)e * 10 + j];
+                if (seen[v]) continue;
+                seen[v] = 1;
+                pro[0].insert(pro[0].end(), {v, t[(size_t)e * 10 + ed[j - 4][0]], t[(size_t)e * 10 + ed[j - 4][1]]});
+            }
+    } else {
+        static const int ed[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {0, 4}, {1, 5}, {2, 6}, {3, 7}, {4, 5}, {5, 6}, {6, 7}, {7, 0}};
+        static const int fc[6][4] = {{0, 1, 2, 3}, {0, 1, 4, 5}, {1, 2, 5, 6}, {2, 3, 6, 7}, {3, 0, 7, 4}, {4, 5, 6, 7}};
+        for (int e = 0; e < E; ++e) {
+            const int32_t* q = t + (size_t)e * 27;
+            for (int k = 0; k < 12; ++k)
+                if (!seen[q[8 + k]]) { seen[q[8 + k]] = 1; pro[0].insert(pro[0].end(), {q[8 + k], q[ed[k][0]], q[ed[k][1]]}); }
+            for (int k = 0; k < 6; ++k)
+                if (!seen[q[20 + k]]) {
+                    seen[q[20 + k]] = 1;
+                    pro[1].insert(pro[1].end(), {q[20 + k], q[fc[k][0]], q[fc[k][1]], q[fc[k][2]], q[fc[k][3]]});
+                }
+            pro[2].push_back(q[26]);
+            for (int j = 0; j < 8; ++j) pro[2].push_back(q[j]);
+        }
+    }
+    const int per[3] = {3, 5, 9};
+    for (int k = 0; k < 3; ++k) {
+        s->n_pro[k] = (int)pro[k].size() / per[k];
+        if (s->n_pro[k] && (st = upload(c, s->mem, s->d_pro[k], pro[k]))) return st;
+    }
+    s->n_mg_map = (int)back.size();
+    return upload(c, s->mem, s->d_mg_map, back);
 }
 
 oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
@@ -550,6 +637,7 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     s->n_nwork = (int)nw.size();
     s->n_fwork = (int)fw.size();
     if ((st = upload(c, s->mem, s->d_nwork, nw)) || (st = upload(c, s->mem, s->d_fwork, fw))) return st;
+    if (d->mg_linear > 0.f) return build_multigrid(c, d, s);
     return OCT_OK;
 }
 
@@ -560,6 +648,15 @@ StepParams base_params(oct_ctx* c, float dt) {
     P.omega = 1.f;
     P.error = c->d_error;
     return P;
+}
+
+void mg_prolong(oct_scene* s, cudaStream_t st) {
+    const int k[3] = {2, 4, 8};
+    const float w[3] = {0.5f, 0.25f, 0.125f};
+    for (int i = 0; i < 3; ++i) {
+        launch_mg_prolong(s->d_scene, s->d_pro[i], s->n_pro[i], k[i], w[i], st);
+        if (s->n_pro[i]) s->ctx->launches++;
+    }
 }
 
 // Scripted effects of one scene, in creation order (each a no-op while inactive).
@@ -589,6 +686,35 @@ void vbd_substep(oct_scene* s, float dt) {
     std::vector<int> order(s->n_colors);
     float omega = 1.f;
     for (int j = 0; j < s->iterations; ++j) {
+        if (s->mg_sub) {
+            // MG_VBD_FEM::solve schedule: mg_max[1] iterations on the linear level, then
+            // mg_max[0] on the full one, counted across sub-steps; entering the linear level
+            // prolongs the mid nodes first
+            const int last = s->mg_current;
+            s->mg_count++;
+            while (s->mg_count > s->mg_max[s->mg_current]) { s->mg_count = 1; s->mg_current = (s->mg_current + 1) % 2; }
+            if (s->mg_current == 1) {
+                if (last != 1) mg_prolong(s, st);
+                oct_scene* L = s->mg_sub;
+                launch_mg_copy(s->d_scene, L->d_scene, s->d_mg_map, s->n_mg_map, 0, st);
+                StepParams PL = P;
+                PL.in_place = L->in_place ? 1 : 0;
+                PL.pending_v0 = nullptr;
+                for (int k = 0; k < L->n_colors; ++k) {
+                    const int b = L->vwork_off[k], n = L->vwork_off[k + 1] - b;
+                    launch_vertex(L->element, L->material, L->d_scene, L->d_vwork + b, n, L->tpv, 0, PL, nullptr, st);
+                    if (!L->in_place) launch_commit(L->d_scene, L->d_vwork + b, n, st);
+                    c->launches += L->in_place ? 1 : 2;
+                }
+                launch_mg_copy(s->d_scene, L->d_scene, s->d_mg_map, s->n_mg_map, 1, st);
+                c->launches += 2;
+                if (s->n_fixed) { launch_constraints(s->d_scene, s->d_fwork, s->n_fwork, 0, st); c->launches++; }
+                enqueue_effects(s, dt, st);
+                if (s->box) { launch_constraints(s->d_scene, s->d_nwork, s->n_nwork, 1, st); c->launches++; }
+                mg_prolong(s, st);   // MG_VertexBlockDescent::step interpolates after every iteration
+                continue;
+            }
+        }
         std::iota(order.begin(), order.end(), 0);
         if (s->order_mode == OCT_ORDER_SHUFFLED) std::shuffle(order.begin(), order.end(), s->rng);
         for (int k : order) {
@@ -694,6 +820,7 @@ void oct_desc_init(oct_scene_desc* d) {
     d->color_algo = OCT_COLOR_DSAT;
     d->precision = OCT_PREC_PLAIN;
     d->xpbd_version = OCT_XPBD_OPTISHARED;
+    d->mg_linear = 0.f;
     for (int k = 0; k < 3; ++k) { d->box_min[k] = -1e30f; d->box_max[k] = 1e30f; }
 }
 
@@ -767,6 +894,7 @@ oct_status oct_scene_create(oct_ctx* c, const oct_scene_desc* d, oct_scene** out
 oct_status oct_scene_destroy(oct_scene* s) {
     if (!s) return OCT_EINVAL;
     cudaStreamSynchronize(s->ctx->stream);
+    if (s->mg_sub) oct_scene_destroy(s->mg_sub);
     drop_frame_graph(s);
     s->mem.release();
     delete s;
@@ -780,7 +908,7 @@ oct_status oct_scene_step(oct_scene* s, float frame_dt, int substeps) {
     s->last_substeps = substeps;
     // the first frame after set-up (pending initial velocity) and shuffled colour orders run
     // launch by launch; otherwise a captured frame is replayed
-    const bool graph = s->capture && s->order_mode != OCT_ORDER_SHUFFLED && !s->pending_host;
+    const bool graph = s->capture && s->order_mode != OCT_ORDER_SHUFFLED && !s->pending_host && !s->mg_sub;
     if (graph && (!s->frame_exec || s->frame_dt != frame_dt || s->frame_substeps != substeps)) {
         drop_frame_graph(s);
         const uint64_t l0 = c->launches;
@@ -1135,6 +1263,7 @@ oct_status oct_batch_create(oct_ctx* c, oct_scene* const* scenes, int n, oct_bat
         if (s->solver != OCT_SOLVER_VBD) return fail(c, OCT_ENOTSUP, "batches hold VBD scenes");
         if (s->iterations != b->iterations || s->rho != b->rho) return fail(c, OCT_ENOTSUP, "batch scenes need equal iterations and rho");
         if (s->order_mode != OCT_ORDER_ASCENDING) return fail(c, OCT_ENOTSUP, "batches use the ascending colour order");
+        if (s->mg_sub) return fail(c, OCT_ENOTSUP, "multigrid scenes are stepped alone");
         b->scenes.push_back(s);
         hs.push_back(s->h);
         b->pending_host.push_back(s->pending_host);

@@ -766,9 +766,21 @@ template <class T> void scene_energy(const Fem<T>& f, const State<T>& s, double*
 }
 
 // ----------------------------------------------------------------------------- GPU-semantics VBD
+// Owner lists: per node, (element, local index) in element order.
+using Owners = std::vector<std::vector<std::pair<int, int>>>;
+
 template <class T> struct VBD {
     Fem<T> fem;
     State<T> s;
+    // multigrid (MG_VBD_FEM, MG_VertexBlockDescent.cpp:134-239): level 1 is the linear mesh of
+    // the corners, solved with its own colouring and masses; mid nodes follow by prolongation
+    bool mg = false;
+    int max_it[2] = {0, 0}, it_count = 0, current = 1;
+    Fem<T> fem_lin;
+    std::vector<std::vector<int>> by_color_lin;
+    Owners owners_lin;
+    std::vector<T> m_lin;
+    std::vector<int> pro_edge, pro_face, pro_vol;   // (id, 2 / 4 / 8 corner ids) per entry
     int iterations = 1;
     T rho = 0, damping = 0;
     bool in_place = false;
@@ -781,18 +793,24 @@ template <class T> struct VBD {
     bool has_v0 = false;
 };
 
+template <class T> void vbd_vertex(const Fem<T>& f, const Owners& owners, const State<T>& s, int vid, T dt, V3<T>& fi,
+                                   M3<T>& H);
 template <class T> void vbd_vertex(VBD<T>& b, int vid, T dt, V3<T>& fi, M3<T>& H) {
+    vbd_vertex(b.fem, b.owners, b.s, vid, dt, fi, H);
+}
+template <class T> void vbd_vertex(const Fem<T>& f, const Owners& owners, const State<T>& s, int vid, T dt, V3<T>& fi,
+                                   M3<T>& H) {
     // kernel_vbd_solve_v3/v4 body: per (owner, qp) compute_f_H_sym (GPU_VBD_FEM.cu:42-63),
     // summed over the vertex's owners in element order and its quadrature points.
-    const Fem<T>& f = b.fem;
+    (void)dt;
     fi = V3<T>();
     H = M3<T>(T(0));
-    for (auto [eid, r] : b.owners[vid])
+    for (auto [eid, r] : owners[vid])
         for (int q = 0; q < f.nq; ++q) {
             const M3<T>& Ji = f.JX_inv[eid * f.nq + q];
             const T V = f.V[eid * f.nq + q];
             M3<T> Jx(T(0));
-            for (int i = 0; i < f.ne; ++i) Jx = Jx + outer(b.s.p[f.topo[eid * f.ne + i]], f.dN[q * f.ne + i]);
+            for (int i = 0; i < f.ne; ++i) Jx = Jx + outer(s.p[f.topo[eid * f.ne + i]], f.dN[q * f.ne + i]);
             const M3<T> F = Jx * Ji;
             const V3<T> g = transpose(Ji) * f.dN[q * f.ne + r];
             const M3<T> P = pk1(f.material, f.lambda[eid], f.mu[eid], F);
@@ -804,14 +822,30 @@ template <class T> void vbd_vertex(VBD<T>& b, int vid, T dt, V3<T>& fi, M3<T>& H
 }
 
 // compute_correction (GPU_VBD_FEM.cu:107-122)
-template <class T> V3<T> vbd_correction(const State<T>& s, int vid, T damping, T dt, V3<T> fi, M3<T> H) {
+template <class T> V3<T> vbd_correction(const State<T>& s, int vid, T damping, T dt, V3<T> fi, M3<T> H, T mass = T(-1)) {
     fi = fi - (damping / dt) * H * (s.p[vid] - s.last_p[vid]);
     H = H + (damping / dt) * H;
-    const T mh2 = s.m[vid] / (dt * dt);
+    const T mh2 = (mass >= T(0) ? mass : s.m[vid]) / (dt * dt);
     fi = fi - mh2 * (s.p[vid] - s.y[vid]);
     H[0][0] += mh2; H[1][1] += mh2; H[2][2] += mh2;
     const T dH = std::abs(det(H));
     return dH > T(1e-6f) ? inverse(H) * fi : V3<T>();
+}
+
+// P1_to_P2 / Q1_to_Q2::prolongation (MG_VertexBlockDescent.cpp:37-96): each mid node moves by
+// the mean displacement since the sub-step start of its edge / face / element corners.
+template <class T> void mg_prolong(VBD<T>& b) {
+    State<T>& s = b.s;
+    auto apply = [&](const std::vector<int>& list, int k, T w) {
+        for (size_t i = 0; i < list.size(); i += k + 1) {
+            V3<T> d;
+            for (int j = 1; j <= k; ++j) d = d + (s.p[list[i + j]] - s.last_p[list[i + j]]);
+            s.p[list[i]] = s.last_p[list[i]] + d * w;
+        }
+    };
+    apply(b.pro_edge, 2, T(0.5f));
+    apply(b.pro_face, 4, T(0.25f));
+    apply(b.pro_vol, 8, T(0.125f));
 }
 
 // GPU_VBD::step (GPU_VBD.cu:38-61) + GPU_VBD_FEM::step (GPU_VBD_FEM.cu:712-755) for one
@@ -832,28 +866,45 @@ template <class T> void vbd_substep(VBD<T>& b, T dt) {
     T omega = 1;
     std::vector<int> order(b.n_colors);
     for (int j = 0; j < b.iterations; ++j) {
+        // multigrid schedule (MG_VBD_FEM::solve): max_it[1] iterations on the linear level,
+        // then max_it[0] on the full one, counted across sub-steps; entering the linear level
+        // prolongs the mid nodes first
+        int level = 0;
+        if (b.mg) {
+            const int last = b.current;
+            b.it_count++;
+            while (b.it_count > b.max_it[b.current]) { b.it_count = 1; b.current = (b.current + 1) % 2; }
+            level = b.current;
+            if (last != level && level == 1) mg_prolong(b);
+        }
+        const Fem<T>& fl = level ? b.fem_lin : b.fem;
+        const Owners& ol = level ? b.owners_lin : b.owners;
+        const auto& colours = level ? b.by_color_lin : b.by_color;
+        const bool in_place = level ? true : b.in_place;
+        order.resize(colours.size());
         std::iota(order.begin(), order.end(), 0);
         if (b.order_mode == 1) std::shuffle(order.begin(), order.end(), b.rng);
         for (int c : order) {
-            const std::vector<int>& vs = b.by_color[c];
-            if (b.in_place) {
+            const std::vector<int>& vs = colours[c];
+            if (in_place) {
                 for (int vid : vs) {
                     if (s.mask[vid] == 0) continue;
                     V3<T> fi; M3<T> H;
-                    vbd_vertex(b, vid, dt, fi, H);
-                    s.p[vid] = s.p[vid] + vbd_correction(s, vid, b.damping, dt, fi, H);
+                    vbd_vertex(fl, ol, s, vid, dt, fi, H);
+                    s.p[vid] = s.p[vid] + vbd_correction(s, vid, b.damping, dt, fi, H, level ? b.m_lin[vid] : T(-1));
                 }
             } else {
                 for (int vid : vs) {
                     if (s.mask[vid] == 0) continue;
                     V3<T> fi; M3<T> H;
-                    vbd_vertex(b, vid, dt, fi, H);
+                    vbd_vertex(fl, ol, s, vid, dt, fi, H);
                     s.p_new[vid] = s.p[vid] + vbd_correction(s, vid, b.damping, dt, fi, H);
                 }
                 for (int vid : vs) if (s.mask[vid] != 0) s.p[vid] = s.p_new[vid];   // kernel_copy_in_position
             }
         }
         apply_constraints(s, dt);
+        if (b.mg && b.current == 1) mg_prolong(b);   // MG_VertexBlockDescent::step: interpolate after each iteration
         if (b.rho > T(0) && b.rho > T(1.17549435e-38f * 1e6f)) {   // GPU_VBD.cu:50-56
             if (j == 1) omega = T(2) / (T(2) - b.rho * b.rho);
             else if (j > 1) omega = T(4) / (T(4) - b.rho * b.rho * omega);
@@ -886,6 +937,69 @@ template <class T> VBD<T>* vbd_create(const orc_desc* d) {
     b->order_mode = d->order_mode;
     b->rng.seed((unsigned)d->seed);
     b->has_v0 = d->initial_velocity != nullptr;
+    if (d->mg_linear > 0.f) {
+        if ((d->element != Tetra10 && d->element != Hexa27) || !d->mg_masses) { delete b; return nullptr; }
+        const int nl = d->element == Tetra10 ? 4 : 8, ne = b->fem.ne, E = d->n_elements;
+        const int it_lin = (int)((float)d->iterations * d->mg_linear);
+        b->mg = true;
+        b->max_it[0] = d->iterations - it_lin;
+        b->max_it[1] = it_lin;
+        std::vector<int32_t> lin((size_t)E * nl);
+        for (int e = 0; e < E; ++e) for (int j = 0; j < nl; ++j) lin[(size_t)e * nl + j] = d->topology[(size_t)e * ne + j];
+        orc_desc dl = *d;
+        dl.element = d->element == Tetra10 ? Tetra : Hexa;
+        dl.topology = lin.data();
+        if (!build_fem(&dl, b->fem_lin)) { delete b; return nullptr; }
+        // colouring of the corner graph: DSAT on the corners numbered in ascending order
+        std::vector<int> compact(d->n_nodes, -1), back;
+        for (int32_t v : lin) compact[v] = 0;
+        for (int i = 0; i < d->n_nodes; ++i) if (compact[i] == 0) { compact[i] = (int)back.size(); back.push_back(i); }
+        std::vector<int32_t> lc(lin.size());
+        for (size_t k = 0; k < lin.size(); ++k) lc[k] = compact[lin[k]];
+        Graph g = build_primal(nl, lc.data(), E);
+        std::vector<int> col;
+        const int nc = dsat(g, col);
+        b->by_color_lin.assign(nc, {});
+        for (size_t k = 0; k < back.size(); ++k) b->by_color_lin[col[k]].push_back(back[k]);
+        b->owners_lin.assign(d->n_nodes, {});
+        for (int e = 0; e < E; ++e) for (int j = 0; j < nl; ++j) b->owners_lin[lin[(size_t)e * nl + j]].push_back({e, j});
+        b->m_lin.assign(d->n_nodes, T(0));
+        for (int i = 0; i < d->n_nodes; ++i) b->m_lin[i] = (T)d->mg_masses[i];
+        // prolongation lists, first visit in element order (P1_to_P2 / Q1_to_Q2 constructors)
+        std::vector<char> seen(d->n_nodes, 0);
+        const int* t = d->topology;
+        if (d->element == Tetra10) {
+            static const int ed[6][2] = {{0, 1}, {1, 2}, {2, 0}, {0, 3}, {1, 3}, {2, 3}};
+            for (int e = 0; e < E; ++e)
+                for (int j = 4; j < 10; ++j) {
+                    const int v = t[e * 10 + j];
+                    if (seen[v]) continue;
+                    seen[v] = 1;
+                    b->pro_edge.insert(b->pro_edge.end(), {v, t[e * 10 + ed[j - 4][0]], t[e * 10 + ed[j - 4][1]]});
+                }
+        } else {
+            // the reference's edge list ends with {7, 0} for node 19 (the edge is 7-4)
+            static const int ed[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {0, 4}, {1, 5}, {2, 6}, {3, 7}, {4, 5}, {5, 6}, {6, 7}, {7, 0}};
+            static const int fc[6][4] = {{0, 1, 2, 3}, {0, 1, 4, 5}, {1, 2, 5, 6}, {2, 3, 6, 7}, {3, 0, 7, 4}, {4, 5, 6, 7}};
+            for (int e = 0; e < E; ++e) {
+                const int* c = t + (size_t)e * 27;
+                for (int k = 0; k < 12; ++k) {
+                    const int v = c[8 + k];
+                    if (seen[v]) continue;
+                    seen[v] = 1;
+                    b->pro_edge.insert(b->pro_edge.end(), {v, c[ed[k][0]], c[ed[k][1]]});
+                }
+                for (int k = 0; k < 6; ++k) {
+                    const int v = c[20 + k];
+                    if (seen[v]) continue;
+                    seen[v] = 1;
+                    b->pro_face.insert(b->pro_face.end(), {v, c[fc[k][0]], c[fc[k][1]], c[fc[k][2]], c[fc[k][3]]});
+                }
+                b->pro_vol.push_back(c[26]);
+                for (int j = 0; j < 8; ++j) b->pro_vol.push_back(c[j]);
+            }
+        }
+    }
     return b;
 }
 

@@ -52,6 +52,10 @@ typedef struct orc_desc {
     /* XPBD */
     float global_damping;
     int32_t xpbd_version;     /* XPBD_FEM_VERSION: 0 XPBD, 1 Quadrature, 2 OptiShared, 3 OptiGroup */
+    /* multigrid VBD (P2 / Q2 only): fraction of the iterations on the linear corner mesh, and
+     * the node masses of that linear mesh (n_nodes; corner entries used); 0 = off */
+    float mg_linear;
+    const float* mg_masses;
 } orc_desc;
 
 int orc_elem_nodes(int element);

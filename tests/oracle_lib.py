@@ -28,6 +28,7 @@ class OrcDesc(C.Structure):
         ("colors", C.POINTER(C.c_int32)), ("order_mode", C.c_int32), ("seed", C.c_uint64),
         ("box_limit", C.c_int32), ("box_min", C.c_float * 3), ("box_max", C.c_float * 3),
         ("global_damping", C.c_float), ("xpbd_version", C.c_int32),
+        ("mg_linear", C.c_float), ("mg_masses", C.POINTER(C.c_float)),
     ]
 
 
@@ -162,13 +163,14 @@ class Scene:
     def __init__(self, element, X, T, m, material=STABLE_NEOHOOKE, young=1e5, poisson=0.45, damping=0.0,
                  gravity=(0, 0, -9.81), fixed=(), v0=None, iterations=20, rho=0.0, in_place=False, colors=None,
                  n_colors=0, order_mode=0, seed=0, young_per_element=None, box=None, global_damping=0.0,
-                 fixed_group=None, xpbd_version=2):
+                 fixed_group=None, xpbd_version=2, mg_linear=0.0, mg_masses=None):
         self.arrays = dict(X=np.ascontiguousarray(X, np.float32), T=np.ascontiguousarray(T, np.int32),
                            m=np.ascontiguousarray(m, np.float32), fixed=np.ascontiguousarray(fixed, np.int32),
                            v0=None if v0 is None else np.ascontiguousarray(v0, np.float32),
                            colors=None if colors is None else np.ascontiguousarray(colors, np.int32),
                            ype=None if young_per_element is None else np.ascontiguousarray(young_per_element, np.float32),
-                           fgroup=None if fixed_group is None else np.ascontiguousarray(fixed_group, np.int32))
+                           fgroup=None if fixed_group is None else np.ascontiguousarray(fixed_group, np.int32),
+                           mgm=None if mg_masses is None else np.ascontiguousarray(mg_masses, np.float32))
         a = self.arrays
         d = OrcDesc()
         d.element = element
@@ -200,6 +202,8 @@ class Scene:
             d.box_max = (C.c_float * 3)(*box[1])
         d.global_damping = global_damping
         d.xpbd_version = xpbd_version
+        d.mg_linear = mg_linear
+        d.mg_masses = _p(a["mgm"], C.c_float)
         self.desc = d
         self.n = d.n_nodes
 
