@@ -712,6 +712,10 @@ def main():
         its = 4 if args.workload == "batched" else (2 if args.workload == "p2" else iterations)
         v, secs, desc = cpu_reference(specs, iterations, substeps, frame_dt, threads, every, its)
         cpu = {"value": v, "unit": "vertex-iter/s", "cores": threads, "kind": "port", "sample": desc}
+        # the reference's CPU VBD is single-threaded: the same restatement on one thread, on a
+        # smaller sample (every 16th scene of the batched workload)
+        v1, secs1, desc1 = cpu_reference(specs, iterations, substeps, frame_dt, 1, 4 * every, its)
+        cpu["single_thread"] = {"value": v1, "cores": 1, "sample": desc1}
 
     if rank == 0:
         line = {
