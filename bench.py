@@ -48,6 +48,45 @@ sys.path.insert(0, ROOT)
 FRAME_DT = 1.0 / 60.0
 
 
+# ---- replicas over ranks: one process per GPU, no data-path collective; only the timing is
+# combined (max over ranks) and the aggregate counts every rank's work
+def init_ranks(world, local, timeout_s=600):
+    """Process group for the replicas (NCCL on GPUs; gloo when no GPU is visible, for tests)."""
+    if world <= 1:
+        return None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    dist.init_process_group(backend, timeout=timedelta(seconds=timeout_s))
+    return dist
+
+
+def max_over_ranks(x, world):
+    """The largest of the ranks' values (each rank's device-timed milliseconds)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_step, steps, world, max_ms):
+    """Whole-job throughput: every rank's units over the slowest rank's time."""
+    return units_per_step * steps * world / (max_ms * 1e-3)
+
+
+def barrier_ranks(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
 def workload_specs(name, seed):
     """List of scene specs: (element, cells, size, young, poisson, density, gravity, iterations, substeps, dt)."""
     import octopusengine_b200 as ob
@@ -243,11 +282,7 @@ def bench_solver(args, world, rank, local, threads):
                           "cpu_baseline": {"value": v, "unit": unit, "cores": 1, "kind": "port", "sample": desc},
                           "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    init_ranks(world, local)
     torch.cuda.set_device(local)
     import octopusengine_b200 as ob
     from octopusengine_b200 import capi
@@ -265,8 +300,7 @@ def bench_solver(args, world, rank, local, threads):
     torch.cuda.synchronize()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     l0 = ctx.launch_count()
-    if world > 1:
-        torch.distributed.barrier()
+    barrier_ranks(world)
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
         ev[0].record(stream)
@@ -274,16 +308,11 @@ def bench_solver(args, world, rank, local, threads):
             scene.step(frame_dt, substeps, sync=False)
             ev[k + 1].record(stream)
         torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    barrier_ranks(world)
     launches = ctx.launch_count() - l0
     step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
-    total_ms = ev[0].elapsed_time(ev[-1])
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = units * args.steps * world / (total_ms * 1e-3)
+    total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]), world)
+    value = aggregate_rate(units, args.steps, world, total_ms)
     # end to end: positions and velocities in from pinned host memory, positions out, each step
     n = scene.n_nodes
     host_p = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
@@ -539,11 +568,7 @@ def main():
         return
 
     import torch
-    if world > 1:
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    init_ranks(world, local)
     device = local
     torch.cuda.set_device(device)
     import octopusengine_b200 as ob
@@ -574,8 +599,7 @@ def main():
     stream = torch.cuda.ExternalStream(stream_ptr.value, device=device)
 
     def barrier():
-        if world > 1:
-            torch.distributed.barrier()
+        barrier_ranks(world)
 
     cube = bool(specs[0].get("cube"))
     frame = [0]
@@ -605,12 +629,8 @@ def main():
     barrier()
     launches = ctx.launch_count() - launches0
     step_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
-    total_ms = ev[0].elapsed_time(ev[-1])
-    if world > 1:
-        t = torch.tensor([total_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = vit_per_step * args.steps * world / (total_ms * 1e-3)
+    total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]), world)
+    value = aggregate_rate(vit_per_step, args.steps, world, total_ms)
 
     # ---- end to end through the C ABI with pinned host buffers
     n_state = batch.state_size
@@ -627,12 +647,8 @@ def main():
         batch.get_state(host_np)
     e_end.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e_start.elapsed_time(e_end)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = vit_per_step * args.steps * world / (e2e_ms * 1e-3)
+    e2e_ms = max_over_ranks(e_start.elapsed_time(e_end), world)
+    e2e_value = aggregate_rate(vit_per_step, args.steps, world, e2e_ms)
     bytes_state = n_state * 4
 
     # ---- roofline of the dominant kernel (the VBD colour kernel of the heaviest group)

@@ -364,6 +364,19 @@ oct_status oct_torsion_profile(int32_t element, const float* rest, const float* 
                                const int32_t* topology, int32_t n_elements, int32_t samples_per_edge, float beam_length,
                                float* distance, float* angles, int32_t capacity, int32_t* count);
 
+/* Checkpoint / restore of one scene (new; the reference's DataRecorder writes no restorable
+ * state): per node the displacement, the start-of-sub-step displacement, the velocity and the
+ * fixed mask, then the fixation groups, the effects' stretch distances, the multigrid schedule
+ * and the pending initial velocity.  A restored scene continues exactly as the saved one. */
+oct_status oct_scene_state_size(oct_scene* s, size_t* n_floats);
+oct_status oct_scene_save(oct_scene* s, float* out);
+oct_status oct_scene_restore(oct_scene* s, const float* in);
+
+/* Failure-detection probe (new): runs the colour kernels' bounded mbarrier wait on a phase
+ * that never completes, with at most limit (<= 1e6) polls, and returns OCT_ETIMEDOUT through
+ * the context's error word; the context stays usable. */
+oct_status oct_ctx_wait_probe(oct_ctx* ctx, int32_t limit);
+
 /* Measurement helpers.  The context's CUDA stream (cudaStream_t), to record events on it. */
 oct_status oct_ctx_stream(oct_ctx* ctx, void** stream);
 /* Measured FP32 FMA throughput of the device (TFLOP/s) from a register-resident FMA loop. */

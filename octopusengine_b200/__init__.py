@@ -191,6 +191,18 @@ class Scene:
                    self.ctx.handle)
         return e
 
+    def save(self):
+        """Checkpoint of the scene state (oct_scene_save)."""
+        n = C.c_size_t()
+        capi.lib().oct_scene_state_size(self._h, C.byref(n))
+        out = np.zeros(n.value, np.float32)
+        capi.check(capi.lib().oct_scene_save(self._h, capi.ptr(out, C.c_float)), "oct_scene_save", self.ctx.handle)
+        return out
+
+    def restore(self, state):
+        a = np.ascontiguousarray(state, np.float32)
+        capi.check(capi.lib().oct_scene_restore(self._h, capi.ptr(a, C.c_float)), "oct_scene_restore", self.ctx.handle)
+
     def add_effect(self, kind, *params):
         """Scripted effect (capi.EFFECT_*), created inactive; returns its index."""
         idx = C.c_int32()

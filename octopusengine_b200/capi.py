@@ -46,6 +46,7 @@ EXPORTS = [
     "oct_shape_values", "oct_reference_nodes", "oct_mesh_error", "oct_beam_sampler_create", "oct_beam_sampler_info",
     "oct_beam_sampler_error", "oct_beam_sampler_destroy", "oct_flexion_error", "oct_torsion_profile",
     "oct_scene_add_effect", "oct_scene_set_effect_active", "oct_scene_effect_ids", "oct_surface_nodes",
+    "oct_scene_state_size", "oct_scene_save", "oct_scene_restore", "oct_ctx_wait_probe",
 ]
 
 
@@ -129,6 +130,10 @@ def lib():
             "oct_scene_write_vtk": ([vp, C.c_char_p], C.c_int),
             "oct_shape_values": ([C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
             "oct_scene_add_effect": ([vp, C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_int32)], C.c_int),
+            "oct_scene_state_size": ([vp, C.POINTER(C.c_size_t)], C.c_int),
+            "oct_scene_save": ([vp, C.POINTER(C.c_float)], C.c_int),
+            "oct_scene_restore": ([vp, C.POINTER(C.c_float)], C.c_int),
+            "oct_ctx_wait_probe": ([vp, C.c_int32], C.c_int),
             "oct_scene_set_effect_active": ([vp, C.c_int32, C.c_int], C.c_int),
             "oct_scene_effect_ids": ([vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)], C.c_int),
             "oct_surface_nodes": ([C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)],

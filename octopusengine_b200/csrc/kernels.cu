@@ -400,9 +400,9 @@ __device__ __forceinline__ void vertex_epilogue(const SceneDev& S, int vid, cons
 }
 
 // Bounded wait on an mbarrier phase; false when the iteration limit ran out.
-__device__ __forceinline__ bool mbar_wait(unsigned mb, unsigned phase) {
+__device__ __forceinline__ bool mbar_wait(unsigned mb, unsigned phase, long limit = kSpinLimit) {
     unsigned done = 0;
-    for (long it = 0; it < kSpinLimit && !done; ++it)
+    for (long it = 0; it < limit && !done; ++it)
         asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
                      : "=r"(done) : "r"(mb), "r"(phase) : "memory");
     return done != 0;
@@ -788,6 +788,17 @@ __global__ void k_mg_prolong(const SceneDev* __restrict__ main, const int* __res
     }
     const float4 ul = main->u_last[e[0]];
     main->u[e[0]] = make_float4(ul.x + dx * w, ul.y + dy * w, ul.z + dz * w, ul.w);
+}
+
+// Failure-detection probe: one thread waits, through the same bounded mbarrier wait as the
+// colour kernels, on a phase that no copy and no thread will ever complete; when the limit
+// runs out it records the time-out in the context's error word (bit 0) and returns.
+__global__ void k_wait_probe(int* error, long limit) {
+    __shared__ __align__(8) unsigned long long bar;
+    const unsigned mb = (unsigned)__cvta_generic_to_shared(&bar);
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (!mbar_wait(mb, 0, limit)) atomicOr(error, 1);
 }
 
 // Host-state staging of a batch: state[off_s + 3 i ...] = u_i then v_i (n*3 floats each).
@@ -1467,6 +1478,8 @@ void launch_mg_copy(const SceneDev* main, const SceneDev* sub, const int* map, i
 void launch_mg_prolong(const SceneDev* main, const int* list, int count, int k, float w, cudaStream_t st) {
     if (count > 0) k_mg_prolong<<<(count + 255) / 256, 256, 0, st>>>(main, list, count, k, w);
 }
+
+void launch_wait_probe(int* error, long limit, cudaStream_t st) { k_wait_probe<<<1, 1, 0, st>>>(error, limit); }
 
 void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, int box_pass, cudaStream_t st) {
     if (n_work <= 0) return;

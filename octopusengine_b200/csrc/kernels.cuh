@@ -27,6 +27,8 @@ void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, i
 // and the prolongation of mid nodes from k corners with weight w.
 void launch_mg_copy(const SceneDev* main, const SceneDev* sub, const int* map, int n, int dir, cudaStream_t st);
 void launch_mg_prolong(const SceneDev* main, const int* list, int count, int k, float w, cudaStream_t st);
+// Failure-detection probe: a bounded wait on a phase nothing completes (error bit 0 on time-out).
+void launch_wait_probe(int* error, long limit, cudaStream_t st);
 // One scripted effect of one scene (kind 0 crush / 1 random sphere over the node chunks in
 // work, kind 2 high stretch over its ids); a no-op while the effect is inactive.
 void launch_effect(const SceneDev* scene, const NWork* work, int n_work, int slot, int kind, float dt, cudaStream_t st);

@@ -15,6 +15,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/octopus_b200.h"
 #include "device.cuh"
 #include "host.hpp"
@@ -24,6 +26,13 @@ using namespace octb;
 
 namespace {
 constexpr int kBlockThreads = 128;
+
+// NVTX ranges around frames, sub-steps and colour sweeps (host side; a profiler shows them on
+// the timeline, and without one they cost a pointer test).
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+};
 constexpr int kNodeChunk = 256;
 }  // namespace
 
@@ -671,6 +680,7 @@ void enqueue_effects(oct_scene* s, float dt, cudaStream_t st) {
 // launch structure: predictor, iterations x (one launch per colour [+ commit] + constraints
 // [+ Chebyshev]), velocity update.
 void vbd_substep(oct_scene* s, float dt) {
+    Range range("vbd_substep");
     oct_ctx* c = s->ctx;
     cudaStream_t st = c->stream;
     StepParams P = base_params(c, dt);
@@ -717,6 +727,7 @@ void vbd_substep(oct_scene* s, float dt) {
         }
         std::iota(order.begin(), order.end(), 0);
         if (s->order_mode == OCT_ORDER_SHUFFLED) std::shuffle(order.begin(), order.end(), s->rng);
+        Range sweep("colour_sweep");
         for (int k : order) {
             const int b = s->vwork_off[k], n = s->vwork_off[k + 1] - b;
             launch_vertex(s->element, s->material, s->d_scene, s->d_vwork + b, n, s->tpv, 0, P, nullptr, st);
@@ -741,6 +752,7 @@ void vbd_substep(oct_scene* s, float dt) {
 
 // GPU_PBD::step (octopus/src/GPU/PBD/GPU_PBD.cu:20-26).
 void xpbd_substep(oct_scene* s, float dt) {
+    Range range("xpbd_substep");
     oct_ctx* c = s->ctx;
     cudaStream_t st = c->stream;
     StepParams P = base_params(c, dt);
@@ -760,6 +772,7 @@ void xpbd_substep(oct_scene* s, float dt) {
 
 // GPU_SemiExplicit::step (octopus/src/GPU/GPU_Integrator.cu:36-42).
 void explicit_substep(oct_scene* s, float dt) {
+    Range range("explicit_substep");
     oct_ctx* c = s->ctx;
     cudaStream_t st = c->stream;
     StepParams P = base_params(c, dt);
@@ -903,6 +916,7 @@ oct_status oct_scene_destroy(oct_scene* s) {
 
 oct_status oct_scene_step(oct_scene* s, float frame_dt, int substeps) {
     if (!s || substeps <= 0 || !(frame_dt > 0.f)) return OCT_EINVAL;
+    Range range("oct_scene_step");
     oct_ctx* c = s->ctx;
     const float sub = frame_dt / (float)substeps;
     s->last_substeps = substeps;
@@ -1140,6 +1154,84 @@ oct_status oct_surface_nodes(int32_t element, const int32_t* topology, int32_t n
     const std::vector<int32_t> v = surface_nodes(element, topology, n_elements);
     *n = (int32_t)v.size();
     if (ids) std::copy(v.begin(), v.end(), ids);
+    return OCT_OK;
+}
+
+oct_status oct_ctx_wait_probe(oct_ctx* c, int32_t limit) {
+    if (!c || limit <= 0 || limit > 1000000) return OCT_EINVAL;
+    launch_wait_probe(c->d_error, limit, c->stream);
+    OCT_CUDA(c, cudaGetLastError());
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    return check_error_word(c);
+}
+
+// Checkpoint: per node u, u_last, v (9 floats) and the mask, then the fixation table
+// (kFixGroups x 16), the effects' stretch distances (kMaxEffects), the multigrid schedule (3)
+// and the pending initial-velocity flag.
+oct_status oct_scene_state_size(oct_scene* s, size_t* n_floats) {
+    if (!s || !n_floats) return OCT_EINVAL;
+    *n_floats = (size_t)s->n_nodes * 10 + kFixGroups * 16 + kMaxEffects + 4;
+    return OCT_OK;
+}
+
+oct_status oct_scene_save(oct_scene* s, float* out) {
+    if (!s || !out) return OCT_EINVAL;
+    oct_ctx* c = s->ctx;
+    const int N = s->n_nodes;
+    std::vector<float4> u(N), ul(N), v(N);
+    std::vector<int> mask(N);
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    OCT_CUDA(c, cudaMemcpy(u.data(), s->h.u, sizeof(float4) * N, cudaMemcpyDeviceToHost));
+    OCT_CUDA(c, cudaMemcpy(ul.data(), s->h.u_last, sizeof(float4) * N, cudaMemcpyDeviceToHost));
+    OCT_CUDA(c, cudaMemcpy(v.data(), s->h.v, sizeof(float4) * N, cudaMemcpyDeviceToHost));
+    OCT_CUDA(c, cudaMemcpy(mask.data(), s->h.mask, sizeof(int) * N, cudaMemcpyDeviceToHost));
+    float* o = out;
+    for (int i = 0; i < N; ++i) {
+        *o++ = u[i].x; *o++ = u[i].y; *o++ = u[i].z;
+        *o++ = ul[i].x; *o++ = ul[i].y; *o++ = ul[i].z;
+        *o++ = v[i].x; *o++ = v[i].y; *o++ = v[i].z;
+        *o++ = (float)mask[i];
+    }
+    std::copy(s->fix_host, s->fix_host + kFixGroups * 16, o);
+    o += kFixGroups * 16;
+    for (int k = 0; k < kMaxEffects; ++k) {
+        float t = 0.f;
+        if (k < s->n_effects && s->effects[k].kind == OCT_EFFECT_HIGH_STRETCH)
+            OCT_CUDA(c, cudaMemcpy(&t, s->effects[k].t, sizeof(float), cudaMemcpyDeviceToHost));
+        *o++ = t;
+    }
+    *o++ = (float)s->mg_count; *o++ = (float)s->mg_current; *o++ = (float)s->pending_host; *o++ = 0.f;
+    return OCT_OK;
+}
+
+oct_status oct_scene_restore(oct_scene* s, const float* in) {
+    if (!s || !in) return OCT_EINVAL;
+    oct_ctx* c = s->ctx;
+    const int N = s->n_nodes;
+    std::vector<float4> u(N), ul(N), v(N);
+    std::vector<int> mask(N);
+    const float* p = in;
+    for (int i = 0; i < N; ++i, p += 10) {
+        u[i] = make_float4(p[0], p[1], p[2], 0.f);
+        ul[i] = make_float4(p[3], p[4], p[5], 0.f);
+        v[i] = make_float4(p[6], p[7], p[8], 0.f);
+        mask[i] = p[9] != 0.f ? 1 : 0;
+    }
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    OCT_CUDA(c, cudaMemcpy(s->h.u, u.data(), sizeof(float4) * N, cudaMemcpyHostToDevice));
+    OCT_CUDA(c, cudaMemcpy(s->h.u_last, ul.data(), sizeof(float4) * N, cudaMemcpyHostToDevice));
+    OCT_CUDA(c, cudaMemcpy(s->h.v, v.data(), sizeof(float4) * N, cudaMemcpyHostToDevice));
+    OCT_CUDA(c, cudaMemcpy(s->h.mask, mask.data(), sizeof(int) * N, cudaMemcpyHostToDevice));
+    std::copy(p, p + kFixGroups * 16, s->fix_host);
+    OCT_CUDA(c, cudaMemcpy(s->d_fix, s->fix_host, sizeof(float) * kFixGroups * 16, cudaMemcpyHostToDevice));
+    p += kFixGroups * 16;
+    for (int k = 0; k < kMaxEffects; ++k, ++p)
+        if (k < s->n_effects && s->effects[k].kind == OCT_EFFECT_HIGH_STRETCH)
+            OCT_CUDA(c, cudaMemcpy(s->effects[k].t, p, sizeof(float), cudaMemcpyHostToDevice));
+    s->mg_count = (int)p[0];
+    s->mg_current = (int)p[1];
+    s->pending_host = (int)p[2];
+    OCT_CUDA(c, cudaMemcpy(s->d_pending, &s->pending_host, sizeof(int), cudaMemcpyHostToDevice));
     return OCT_OK;
 }
 
@@ -1384,6 +1476,7 @@ oct_status oct_batch_prepare(oct_batch* b, float frame_dt, int substeps) {
 
 oct_status oct_batch_step(oct_batch* b, float frame_dt, int substeps) {
     if (!b || substeps <= 0 || !(frame_dt > 0.f)) return OCT_EINVAL;
+    Range range("oct_batch_step");
     oct_ctx* c = b->ctx;
     oct_status st = oct_batch_prepare(b, frame_dt, substeps);
     if (st) return st;
