@@ -48,6 +48,11 @@ struct oct_ctx {
     bool tables[10] = {false};
     std::mutex mu;       // guards the budget accounting and the shape-table upload
     std::mutex err_mu;   // guards err (scenes may be created from several host threads)
+    // device blocks released by destroyed scenes and batches, kept for reuse (size -> pointer):
+    // a request loop creates and destroys scenes every few frames, and cudaMalloc / cudaFree
+    // synchronise the device
+    std::multimap<size_t, void*> cache;
+    size_t cached = 0;
 };
 
 namespace {
@@ -67,17 +72,49 @@ oct_status fail(oct_ctx* c, oct_status s, const std::string& msg) {
     } while (0)
 
 // Device allocation accounted against the context budget.
+// Frees every cached block (caller holds ctx->mu).
+void trim_cache(oct_ctx* c) {
+    for (auto& kv : c->cache) cudaFree(kv.second);
+    c->cache.clear();
+    c->cached = 0;
+}
+
+// Device allocation accounted against the context budget.  Released blocks go to the
+// context's cache and are handed out again for requests of at most their size and more than
+// half of it; the budget counts blocks in use plus cached ones, and the cache is trimmed
+// before a request would exceed it.  A scene or batch is released only after the context's
+// stream has drained, so no kernel still reads a block when it is reused.
 struct DevMem {
     oct_ctx* ctx = nullptr;
     std::vector<std::pair<void*, size_t>> blocks;
     template <class T> oct_status alloc(T*& p, size_t n) {
-        const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+        const size_t bytes = ((std::max<size_t>(n, 1) * sizeof(T) + 255) / 256) * 256;
         std::lock_guard<std::mutex> lock(ctx->mu);
+        auto it = ctx->cache.lower_bound(bytes);
+        if (it != ctx->cache.end() && it->first <= 2 * bytes) {
+            p = (T*)it->second;
+            blocks.push_back({it->second, it->first});
+            ctx->used += it->first;
+            ctx->cached -= it->first;
+            ctx->cache.erase(it);
+            return OCT_OK;
+        }
+        while (ctx->used + ctx->cached + bytes > ctx->budget && !ctx->cache.empty()) {
+            auto big = std::prev(ctx->cache.end());
+            cudaFree(big->second);
+            ctx->cached -= big->first;
+            ctx->cache.erase(big);
+        }
         if (ctx->used + bytes > ctx->budget)
             return fail(ctx, OCT_ENOMEM_BUDGET, "HBM budget exceeded: need " + std::to_string(ctx->used + bytes) +
                                                     " bytes, budget " + std::to_string(ctx->budget));
         void* q = nullptr;
         cudaError_t e = cudaMalloc(&q, bytes);
+        if (e == cudaErrorMemoryAllocation && !ctx->cache.empty()) {   // device full of cached blocks
+            cudaGetLastError();
+            trim_cache(ctx);
+            e = cudaMalloc(&q, bytes);
+        }
         if (e != cudaSuccess) return fail(ctx, OCT_ECUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
         blocks.push_back({q, bytes});
         ctx->used += bytes;
@@ -86,7 +123,11 @@ struct DevMem {
     }
     void release() {
         std::lock_guard<std::mutex> lock(ctx->mu);
-        for (auto& b : blocks) { cudaFree(b.first); ctx->used -= b.second; }
+        for (auto& b : blocks) {
+            ctx->used -= b.second;
+            ctx->cache.emplace(b.second, b.first);
+            ctx->cached += b.second;
+        }
         blocks.clear();
     }
 };
@@ -862,6 +903,10 @@ oct_status oct_ctx_create(int device, size_t budget, oct_ctx** out) {
 oct_status oct_ctx_destroy(oct_ctx* c) {
     if (!c) return OCT_EINVAL;
     cudaStreamSynchronize(c->stream);
+    {
+        std::lock_guard<std::mutex> lock(c->mu);
+        trim_cache(c);
+    }
     cudaFree(c->d_error);
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
