@@ -511,6 +511,16 @@ def bench_served(args, threads):
     ctx.close()
 
 
+def vertex_kernel_label(group, scenes):
+    """Name of the colour kernel a batch group launches (its element's lane mapping in effect)."""
+    tpv = next((s.mapping() for s in scenes if s.element == group["element"]), 0)
+    if tpv == -1:
+        return "k_vertex_packed<%d,%d> (VBD colour sweep, element %d, one lane per (vertex, owner) pair)" % (
+            group["element"], group["material"], group["element"])
+    return "k_vertex<%d,%d> (VBD colour sweep, element %d, %d lanes per vertex)" % (
+        group["element"], group["material"], group["element"], tpv)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -661,8 +671,8 @@ def main():
         if capi.lib().oct_batch_group_info(batch._h, g, C.byref(el), C.byref(mat), C.byref(fl), C.byref(by),
                                            C.byref(nl), C.byref(nv)) != 0:
             break
-        groups.append(dict(g=g, element=el.value, flops=fl.value, bytes=by.value, launches=nl.value,
-                           vertices=nv.value))
+        groups.append(dict(g=g, element=el.value, material=mat.value, flops=fl.value, bytes=by.value,
+                           launches=nl.value, vertices=nv.value))
         g += 1
     dom = max(groups, key=lambda x: x["flops"])
     sweeps = 10
@@ -698,7 +708,7 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
                 "frac": achieved_gbs / hbm_peak, "traffic": traffic,
                 "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peaks else "fallback 6650 GB/s",
-                "kernel": "k_vertex<%d,3> (VBD colour sweep, element %d)" % (dom["element"], dom["element"]),
+                "kernel": vertex_kernel_label(dom, scenes),
                 "binding_roof": "fp32",
                 "fp32": {"achieved_tflops": achieved_tflops, "peak_tflops": fp32_peak.value,
                          "frac": achieved_tflops / fp32_peak.value,

@@ -224,6 +224,9 @@ oct_status oct_scene_vertex_residuals(oct_scene* s, float dt, float* out_n3);
  * oct_scene_desc.threads_per_vertex: -1 packed pairs, 0 measured default, 1..32 lanes per
  * vertex).  OCT_ENOTSUP for the packed mapping when a vertex has more than 32 owners. */
 oct_status oct_scene_set_mapping(oct_scene* s, int threads_per_vertex);
+/* The mapping in effect: -1 packed pairs, else lanes per vertex (the measured default and the
+ * fallback for vertices with more than 32 owners resolved); 0 for XPBD scenes. */
+oct_status oct_scene_get_mapping(oct_scene* s, int32_t* threads_per_vertex);
 /* Mapping autotuner (new): for each element type among the scenes, times one colour sweep of
  * all its scenes under every candidate mapping (packed pairs, 1, 2, 4, 8, 16, 32 lanes per
  * vertex) and sets the fastest on those scenes.  The timed sweeps write only the Jacobi

@@ -132,6 +132,12 @@ class Scene:
         capi.check(capi.lib().oct_scene_set_mapping(self._h, int(threads_per_vertex)), "oct_scene_set_mapping",
                    self.ctx.handle)
 
+    def mapping(self):
+        """Lane mapping in effect (-1 packed, else lanes per vertex; 0 for XPBD scenes)."""
+        t = C.c_int32()
+        capi.check(capi.lib().oct_scene_get_mapping(self._h, C.byref(t)), "oct_scene_get_mapping", self.ctx.handle)
+        return t.value
+
     def set_capture(self, on=True):
         """Replay each frame's sub-steps from a captured CUDA graph (oct_scene_set_capture)."""
         capi.check(capi.lib().oct_scene_set_capture(self._h, int(on)), "oct_scene_set_capture", self.ctx.handle)

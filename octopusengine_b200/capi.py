@@ -40,7 +40,7 @@ EXPORTS = [
     "oct_batch_group_info", "oct_batch_time_group", "oct_scene_set_precision", "oct_scene_footprint",
     "oct_server_create", "oct_server_submit", "oct_server_tick", "oct_server_poll", "oct_server_get_stats",
     "oct_server_destroy", "oct_elastic_energy_noalloc", "oct_scene_set_fixation_group",
-    "oct_scene_element_data", "oct_scene_vertex_residuals", "oct_scene_set_mapping", "oct_autotune_mapping",
+    "oct_scene_element_data", "oct_scene_vertex_residuals", "oct_scene_set_mapping", "oct_scene_get_mapping", "oct_autotune_mapping",
     "oct_batch_prepare", "oct_scene_element_type", "oct_scene_get_rest_positions", "oct_scene_get_topology",
     "oct_scene_metadata_json", "oct_vtk_write", "oct_vtk_read_mesh", "oct_vtk_read_field", "oct_scene_write_vtk",
     "oct_shape_values", "oct_reference_nodes", "oct_mesh_error", "oct_beam_sampler_create", "oct_beam_sampler_info",
@@ -117,6 +117,7 @@ def lib():
             "oct_scene_set_capture": ([vp, C.c_int], C.c_int),
             "oct_scene_element_data": ([vp, C.c_int, C.POINTER(C.c_float)], C.c_int),
             "oct_scene_set_mapping": ([vp, C.c_int], C.c_int),
+            "oct_scene_get_mapping": ([vp, ip], C.c_int),
             "oct_batch_prepare": ([vp, C.c_float, C.c_int], C.c_int),
             "oct_scene_element_type": ([vp, C.POINTER(C.c_int32)], C.c_int),
             "oct_scene_get_rest_positions": ([vp, C.POINTER(C.c_float)], C.c_int),

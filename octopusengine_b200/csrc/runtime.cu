@@ -1614,6 +1614,12 @@ oct_status oct_scene_set_mapping(oct_scene* s, int tpv) {
     return build_vertex_work(s);
 }
 
+oct_status oct_scene_get_mapping(oct_scene* s, int32_t* threads_per_vertex) {
+    if (!s || !threads_per_vertex) return OCT_EINVAL;
+    *threads_per_vertex = s->solver == OCT_SOLVER_XPBD ? 0 : (s->tpv == 0 ? -1 : s->tpv);
+    return OCT_OK;
+}
+
 // Times one colour sweep of every group of a batch with the solve results written to the
 // Jacobi buffer (u_new) and not committed, so the scenes' state is left as it was.
 static oct_status time_batch_sweeps(oct_batch* b, int sweeps, float dt, float* ms) {

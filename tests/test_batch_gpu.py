@@ -96,6 +96,7 @@ def test_autotune_keeps_state_and_picks_a_valid_mapping(ctx):
         r = ob.Scene(ctx, e, X, T, **kw)
         r.step(1 / 60, 2)
         r.set_mapping(chosen[e])
+        assert r.mapping() == chosen[e]
         ref.append(r)
     batch = ob.Batch(ctx, tuned)
     rbatch = ob.Batch(ctx, ref)
@@ -111,7 +112,9 @@ def test_set_mapping_mid_run_matches_oracle(ctx, mapping):
     s, o32, o64, mesh = pair(ctx, O.TETRA10, cells=(4, 2, 2), iterations=6)
     s.step(1 / 60, 2)
     o64.step(1 / 60, 2)
+    assert s.mapping() == 2   # the measured default for P2
     s.set_mapping(mapping)
+    assert s.mapping() == mapping
     s.set_capture(True)
     for _ in range(2):
         s.step(1 / 60, 2)
