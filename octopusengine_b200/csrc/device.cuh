@@ -99,6 +99,14 @@ template <int NE> struct EntryLayout {
     static constexpr int kIds = 0, kR = NE, kEid = NE + 1, kRec = NE + 2;
     static constexpr int kWords = ((NE + 2 + 12) + 3) / 4 * 4;
 };
+// P1 (one quadrature point, always affine) entries are 64 B: the node ids with the vertex's
+// own node first, then G_j = JX_inv^T dN_j of the three other nodes in that order (9 floats),
+// V, lambda, mu.  Since sum_i dN_i = 0, F = I + sum_j (u_j - u_own) (x) G_j and the vertex's
+// own g = -(G_1 + G_2 + G_3): no local index, element id or JX_inv needed.
+template <> struct EntryLayout<4> {
+    static constexpr int kIds = 0, kG = 4, kV = 13, kLam = 14, kMu = 15;
+    static constexpr int kWords = 16;
+};
 
 // One unit of node-parallel work (predictor, velocity update, Chebyshev).
 struct NWork {

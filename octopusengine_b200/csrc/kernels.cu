@@ -310,6 +310,34 @@ __device__ __forceinline__ void entry_terms(const SceneDev& S, const float* __re
     constexpr int NE = ElemT<E>::NE;
     using L = EntryLayout<NE>;
     const unsigned long long keep = policy_keep(), stream = policy_stream();
+    if constexpr (NE == 4) {   // compact P1 entry: own node first, G_j of the other three
+        const float4 u0 = ld_hint(&S.u[__float_as_int(en[L::kIds])], keep);
+        const float4 u1 = ld_hint(&S.u[__float_as_int(en[L::kIds + 1])], keep);
+        const float4 u2 = ld_hint(&S.u[__float_as_int(en[L::kIds + 2])], keep);
+        const float4 u3 = ld_hint(&S.u[__float_as_int(en[L::kIds + 3])], keep);
+        const V3 d1 = xyz(u1) - xyz(u0), d2 = xyz(u2) - xyz(u0), d3 = xyz(u3) - xyz(u0);
+        const V3 g1 = mk(en[L::kG], en[L::kG + 1], en[L::kG + 2]);
+        const V3 g2 = mk(en[L::kG + 3], en[L::kG + 4], en[L::kG + 5]);
+        const V3 g3 = mk(en[L::kG + 6], en[L::kG + 7], en[L::kG + 8]);
+        // F_b = e_b + sum_j d_j G_j[b]
+        V3 F0 = d1 * g1.x + d2 * g2.x + d3 * g3.x;
+        V3 F1 = d1 * g1.y + d2 * g2.y + d3 * g3.y;
+        V3 F2 = d1 * g1.z + d2 * g2.z + d3 * g3.z;
+        F0.x += 1.f; F1.y += 1.f; F2.z += 1.f;
+        const V3 g = mk(-(g1.x + g2.x + g3.x), -(g1.y + g2.y + g3.y), -(g1.z + g2.z + g3.z));
+        float t[9];
+        material_terms<MAT>(F0, F1, F2, g, en[L::kLam], en[L::kMu], en[L::kV] * wq<E>(0), t);
+        if (mixed) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) kadd(acc[k], cmp[k], t[k]);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) acc[k] += t[k];
+        }
+#pragma unroll
+        for (int k = 3; k < 9; ++k) acc[k] += t[k];
+        return;
+    } else {
     float ux[NE], uy[NE], uz[NE];
 #pragma unroll
     for (int i = 0; i < NE; ++i) {
@@ -329,6 +357,7 @@ __device__ __forceinline__ void entry_terms(const SceneDev& S, const float* __re
         A = ld_hint(rec, stream); B = ld_hint(rec + 1, stream); C = ld_hint(rec + 2, stream);
     }
     element_terms<E, MAT>(ux, uy, uz, r, A, B, C, rec, affine, s_dN, mixed, acc, cmp, stream);
+    }
 }
 
 // Solve of one vertex: damping and inertia terms (compute_correction,
@@ -494,7 +523,8 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<E>::value) k_vertex_packed(c
         int vid = 0;
         bool active = false;
         if (lane < wk.n_pairs) {
-            vid = __float_as_int(en[EntryLayout<NE>::kIds + __float_as_int(en[EntryLayout<NE>::kR])]);
+            if constexpr (NE == 4) vid = __float_as_int(en[EntryLayout<NE>::kIds]);   // own node first
+            else vid = __float_as_int(en[EntryLayout<NE>::kIds + __float_as_int(en[EntryLayout<NE>::kR])]);
             active = mode == 2 || S.mask[vid] != 0;
         }
         float acc[9], cmp[9];

@@ -654,12 +654,32 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     // owner entries in slot order for the packed mapping (EntryLayout in device.cuh)
     h.ent = nullptr;
     {
-        const int EW = ((NE + 2 + 12) + 3) / 4 * 4;
+        const bool p1 = NE == 4;   // compact 64 B P1 entries (EntryLayout<4>)
+        const int EW = p1 ? 16 : ((NE + 2 + 12) + 3) / 4 * 4;
         std::vector<float4> ent((size_t)owners.size() * EW / 4, make_float4(0, 0, 0, 0));
         for (size_t o = 0; o < owners.size(); ++o) {
             float* e = reinterpret_cast<float*>(&ent[o * EW / 4]);
             int32_t* ei = reinterpret_cast<int32_t*>(e);
             const int eid = owners[o] >> kOwnerShift, r = owners[o] & ((1 << kOwnerShift) - 1);
+            if (p1) {
+                // own node first, then the others in element order with G_j = JX_inv^T dN_j
+                // (FP64 from the stored JX_inv columns m_b; dN_j from the shape table)
+                const float* m = reinterpret_cast<const float*>(&eq[(size_t)eid * 3]);
+                ei[0] = topo[(size_t)eid * NE + r];
+                for (int i = 0, j = 1; i < NE; ++i) {
+                    if (i == r) continue;
+                    ei[j] = topo[(size_t)eid * NE + i];
+                    const double* dn = &sh.dN[(size_t)i * 3];
+                    for (int b = 0; b < 3; ++b)
+                        e[4 + 3 * (j - 1) + b] = (float)((double)m[3 * b] * dn[0] + (double)m[3 * b + 1] * dn[1] +
+                                                         (double)m[3 * b + 2] * dn[2]);
+                    ++j;
+                }
+                e[13] = m[9];    // V
+                e[14] = m[10];   // lambda
+                e[15] = m[11];   // mu
+                continue;
+            }
             for (int i = 0; i < NE; ++i) ei[i] = topo[(size_t)eid * NE + i];
             ei[NE] = r;
             ei[NE + 1] = eid;
