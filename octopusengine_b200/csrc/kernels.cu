@@ -227,6 +227,31 @@ __device__ __forceinline__ void material_terms(V3 F0, V3 F1, V3 F2, V3 g, float 
     }
 }
 
+// Hexa8 node signs (Element numbering of the reference: bottom face counter-clockwise, then the
+// top face); its 2x2x2 Gauss points are the same signs over sqrt(3), in the same order.
+__device__ constexpr int kHexSign[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                           {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+struct HexCoef { V3 x, y, z, xy, xz, yz, xyz; };
+
+// Monomial coefficients (times 1/8) of a trilinear field from its 8 nodal values:
+// u = a0 + a_x xi + a_y eta + a_z zeta + a_xy xi eta + a_xz xi zeta + a_yz eta zeta + a_xyz xi eta zeta.
+// Nodes i and i + 4 differ only in z; on each face, (0, 3) and (1, 2) differ only in y.
+__device__ __forceinline__ void hex_q1_coefficients(const float* ux, const float* uy, const float* uz, HexCoef& h) {
+    V3 p[4], m[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const V3 lo = mk(ux[i], uy[i], uz[i]), hi = mk(ux[i + 4], uy[i + 4], uz[i + 4]);
+        p[i] = hi + lo;   // z-even
+        m[i] = hi - lo;   // z-odd
+    }
+    // y stage on each half: x- pair (0, 3), x+ pair (1, 2)
+    const V3 pe0 = p[0] + p[3], po0 = p[3] - p[0], pe1 = p[1] + p[2], po1 = p[2] - p[1];
+    const V3 me0 = m[0] + m[3], mo0 = m[3] - m[0], me1 = m[1] + m[2], mo1 = m[2] - m[1];
+    constexpr float s = 0.125f;
+    h.x = (pe1 - pe0) * s;   h.y = (po1 + po0) * s;   h.xy = (po1 - po0) * s;
+    h.z = (me1 + me0) * s;   h.xz = (me1 - me0) * s;  h.yz = (mo1 + mo0) * s;   h.xyz = (mo1 - mo0) * s;
+}
+
 // f and H contributions of one owner element (all its quadrature points) to its node r,
 // given the element's node displacements and its first quadrature record (A, B, C); for
 // non-affine elements the later records are read from rec.
@@ -237,17 +262,31 @@ __device__ __forceinline__ void element_terms(const float* ux, const float* uy, 
                                               unsigned long long stream) {
     constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ;
     float fs[3] = {0.f, 0.f, 0.f};   // CompensatePerElement: the element's force over its points
+    // Q1: u(xi) is trilinear, so Jx at every point follows from the seven non-constant monomial
+    // coefficients a_m = 1/8 sum_i s_m(i) u_i (three butterfly stages over the node signs)
+    // instead of a dense 8-node contraction per point (hex_q1_coefficients).
+    [[maybe_unused]] HexCoef hc;
+    if constexpr (E == 6) hex_q1_coefficients(ux, uy, uz, hc);
 #pragma unroll (NQ <= 11 ? NQ : 1)
     for (int q = 0; q < NQ; ++q) {
         if (!affine && q > 0) { A = ld_hint(rec + 3 * q, stream); B = ld_hint(rec + 3 * q + 1, stream); C = ld_hint(rec + 3 * q + 2, stream); }
         // Jx columns: Jk = sum_i u_i dN_qi[k]
         V3 J0 = mk(0, 0, 0), J1 = mk(0, 0, 0), J2 = mk(0, 0, 0);
+        if constexpr (E == 6) {
+            // Gauss point q sits at (s_q0, s_q1, s_q2) / sqrt(3), s_q the signs of node q
+            constexpr float c = 0.57735026918962576f;
+            const float xi = c * kHexSign[q][0], et = c * kHexSign[q][1], ze = c * kHexSign[q][2];
+            J0 = hc.x + hc.xy * et + hc.xz * ze + hc.xyz * (et * ze);
+            J1 = hc.y + hc.xy * xi + hc.yz * ze + hc.xyz * (xi * ze);
+            J2 = hc.z + hc.xz * xi + hc.yz * et + hc.xyz * (xi * et);
+        } else {
 #pragma unroll
-        for (int i = 0; i < NE; ++i) {
-            const float d0 = dn<E>(q, i, 0), d1 = dn<E>(q, i, 1), d2 = dn<E>(q, i, 2);
-            J0.x = fmaf(ux[i], d0, J0.x); J0.y = fmaf(uy[i], d0, J0.y); J0.z = fmaf(uz[i], d0, J0.z);
-            J1.x = fmaf(ux[i], d1, J1.x); J1.y = fmaf(uy[i], d1, J1.y); J1.z = fmaf(uz[i], d1, J1.z);
-            J2.x = fmaf(ux[i], d2, J2.x); J2.y = fmaf(uy[i], d2, J2.y); J2.z = fmaf(uz[i], d2, J2.z);
+            for (int i = 0; i < NE; ++i) {
+                const float d0 = dn<E>(q, i, 0), d1 = dn<E>(q, i, 1), d2 = dn<E>(q, i, 2);
+                J0.x = fmaf(ux[i], d0, J0.x); J0.y = fmaf(uy[i], d0, J0.y); J0.z = fmaf(uz[i], d0, J0.z);
+                J1.x = fmaf(ux[i], d1, J1.x); J1.y = fmaf(uy[i], d1, J1.y); J1.z = fmaf(uz[i], d1, J1.z);
+                J2.x = fmaf(ux[i], d2, J2.x); J2.y = fmaf(uy[i], d2, J2.y); J2.z = fmaf(uz[i], d2, J2.z);
+            }
         }
         // JX_inv columns m_b (m_b[k] = row k, column b)
         const V3 m0 = mk(A.x, A.y, A.z), m1 = mk(A.w, B.x, B.y), m2 = mk(B.z, B.w, C.x);
@@ -570,7 +609,6 @@ __global__ void __launch_bounds__(kBlock, LaneMinBlocks<E>::value) k_vertex(cons
     const int lane = threadIdx.x & 31;
     const int glane = lane & (tpv - 1);           // lane within the vertex group
     const int group = threadIdx.x / tpv;          // vertex index within the block
-    const int vpb = kBlock / tpv;
     for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
         const VWork wk = work[w];
         const SceneDev& S = scenes[wk.scene];
