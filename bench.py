@@ -38,6 +38,7 @@ import json
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -152,7 +153,9 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_%d.csv" % device)
+        # raw samples (the JSON line carries their summary); OCTB_CLOCKS_DIR keeps them elsewhere
+        self.path = os.path.join(os.environ.get("OCTB_CLOCKS_DIR", tempfile.gettempdir()),
+                                 "clocks_bench_%d_%d.csv" % (device, os.getpid()))
 
     def __enter__(self):
         try:
