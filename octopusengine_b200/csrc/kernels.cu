@@ -94,6 +94,17 @@ template <int E> __device__ __forceinline__ float wq(int q) {
 constexpr int kBlock = 128;
 constexpr long kSpinLimit = 1L << 22;
 
+// Programmatic dependent launch.  The kernels of a sub-step (predictor, colour sweeps,
+// constraints, Chebyshev, velocity, XPBD colours) are launched with programmatic stream
+// serialisation: each lets the next one launch once all its blocks have started
+// (pdl_trigger), so that launch and the next kernel's data-independent prologue (the TMA
+// staging of the constant dN table) overlap this kernel's tail; pdl_wait() then blocks until
+// the preceding kernel has completed and its writes are visible.  Both are no-ops for a
+// normal launch.  Every kernel launched by launch_pdl calls pdl_wait() before it reads
+// anything a preceding kernel may write.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ------------------------------------------------------------------------ TMA staging
 // One elected thread issues a cp.async.bulk global->shared copy tracked by an mbarrier;
 // every thread waits on the barrier with an iteration limit.  On time-out the kernel
@@ -538,7 +549,8 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<E>::value) k_vertex_packed(c
     };
     const int stride = gridDim.x * WPB;
     int w = blockIdx.x * WPB + warp;
-    if (lane == 0 && w < n_work) issue(w, 0);
+    if (lane == 0 && w < n_work) issue(w, 0);   // work items and entries are static: before the wait
+    pdl_wait();
     unsigned phase0 = 0, phase1 = 0;
     for (int k = 0; w < n_work; ++k, w += stride) {
         const int b = k & 1;
@@ -588,6 +600,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<E>::value) k_vertex_packed(c
         if (active && lane == head) vertex_epilogue(S, vid, acc, mode, P, red);
         __syncwarp();   // buffer b is refilled by the next-but-one issue
     }
+    pdl_trigger();   // after the sweep: the next launch overlaps this kernel's tail only
 }
 
 template <int E> constexpr int packed_smem_bytes() { return (kBlock / 32) * 2 * 32 * EntryLayout<ElemT<E>::NE>::kWords * 4; }
@@ -605,6 +618,7 @@ __global__ void __launch_bounds__(kBlock, LaneMinBlocks<E>::value) k_vertex(cons
     __shared__ __align__(128) float s_dN[((NQ * NE * 3 + 3) / 4) * 4];
     __shared__ __align__(8) unsigned long long s_mbar;
     stage_table(s_dN, gdN<E>(), NQ * NE * 3, &s_mbar, P.error);
+    pdl_wait();
 
     const int lane = threadIdx.x & 31;
     const int glane = lane & (tpv - 1);           // lane within the vertex group
@@ -663,6 +677,7 @@ __global__ void __launch_bounds__(kBlock, LaneMinBlocks<E>::value) k_vertex(cons
         }
         if (active && glane == 0) vertex_epilogue(S, vid, acc, mode, P, red);
     }
+    pdl_trigger();   // after the sweep: the next launch overlaps this kernel's tail only
 }
 
 // ------------------------------------------------------------------------ node kernels
@@ -674,6 +689,8 @@ constexpr int kNodeChunk = 256;
 __global__ void k_predict(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work, int n_work, int kind,
                           int use_force, int chebyshev, StepParams P) {
     (void)n_work;
+    pdl_trigger();
+    pdl_wait();
     const NWork wk = work[blockIdx.x];
     if (threadIdx.x >= wk.count) return;
     const SceneDev& S = scenes[wk.scene];
@@ -709,6 +726,8 @@ __global__ void k_predict(const SceneDev* __restrict__ scenes, const NWork* __re
 // kernel_velocity_update (GPU_VBD.cu:20-25); with global damping for XPBD (GPU_PBD.cu:8-18).
 __global__ void k_velocity(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work, int n_work,
                            float global_damping, int pbd, StepParams P) {
+    pdl_trigger();
+    pdl_wait();
     const NWork wk = work[blockIdx.x];
     if (threadIdx.x >= wk.count) return;
     const SceneDev& S = scenes[wk.scene];
@@ -728,6 +747,8 @@ __global__ void k_velocity(const SceneDev* __restrict__ scenes, const NWork* __r
 
 // Chebyshev semi-iterative acceleration (kernel_chebychev_acceleration, GPU_VBD.cu:27-36).
 __global__ void k_chebyshev(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work, int n_work, StepParams P) {
+    pdl_trigger();
+    pdl_wait();
     const NWork wk = work[blockIdx.x];
     if (threadIdx.x >= wk.count) return;
     const SceneDev& S = scenes[wk.scene];
@@ -745,6 +766,8 @@ __global__ void k_chebyshev(const SceneDev* __restrict__ scenes, const NWork* __
 // Fixed nodes (kernel_constraint_fix, GPU_Constraint.cu:8-20) then, if enabled, the box
 // clamp of free nodes (kernel_constraint_box_limit, :80-92).  One block per scene chunk.
 __global__ void k_constraints(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work, int n_work, int box_pass) {
+    pdl_trigger();
+    pdl_wait();
     const NWork wk = work[blockIdx.x];
     if (threadIdx.x >= wk.count) return;
     const SceneDev& S = scenes[wk.scene];
@@ -913,6 +936,8 @@ void launch_state(const SceneDev* scenes, const NWork* work, int n_work, const l
 
 // Jacobi commit of a colour (kernel_copy_in_position, GPU_VBD_FEM.cu:402-413).
 __global__ void k_commit(const SceneDev* __restrict__ scenes, const VWork* __restrict__ work, int n_work) {
+    pdl_trigger();
+    pdl_wait();
     for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
         const VWork wk = work[w];
         const SceneDev& S = scenes[wk.scene];
@@ -1062,7 +1087,9 @@ __global__ void __launch_bounds__(kBlock) k_xpbd(const SceneDev* __restrict__ sc
     __shared__ __align__(16) float4 s_pos[GPB][NE];
     __shared__ __align__(16) float4 s_P[GPB][NQ][3];
     __shared__ unsigned long long s_mbar;
+    pdl_trigger();
     stage_table(s_dN, gdN<E>(), NQ * NE * 3, &s_mbar, P.error);
+    pdl_wait();
 
     const int lane = threadIdx.x % G, grp = threadIdx.x / G;
     const int t = blockIdx.x * GPB + grp;
@@ -1363,6 +1390,22 @@ __global__ void k_energy_nodes(const SceneDev* __restrict__ scenes, int scene, d
 
 // ------------------------------------------------------------------------ launchers
 namespace {
+// Launch with programmatic stream serialisation (pdl_trigger / pdl_wait in the kernel).
+template <class... P, class... A>
+void launch_pdl(void (*kernel)(P...), unsigned grid, unsigned block, size_t smem, cudaStream_t st, A... args) {
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 template <class K> int persistent_grid(K kernel, int n_work, size_t smem = 0) {
     static int sms = 0;
     if (!sms) {
@@ -1399,13 +1442,13 @@ void vertex_dispatch(const SceneDev* scenes, const VWork* work, int n_work, int 
         int cap = grid_cap<E, MAT, true>();
         if (cap <= 0) cap = 148 * 4;
         const int blocks = (n_work + kBlock / 32 - 1) / (kBlock / 32);
-        k_vertex_packed<E, MAT><<<blocks < cap ? blocks : cap, kBlock, packed_smem_bytes<E>(), st>>>(scenes, work, n_work, mode, P, red);
+        launch_pdl(k_vertex_packed<E, MAT>, blocks < cap ? blocks : cap, kBlock, packed_smem_bytes<E>(), st, scenes, work, n_work, mode, P, red);
         return;
     }
     int cap = grid_cap<E, MAT, false>();
     if (cap <= 0) cap = 148 * 4;
     const int grid = n_work < cap ? n_work : cap;
-    k_vertex<E, MAT><<<grid, kBlock, 0, st>>>(scenes, work, n_work, tpv, mode, P, red);
+    launch_pdl(k_vertex<E, MAT>, grid, kBlock, 0, st, scenes, work, n_work, tpv, mode, P, red);
 }
 
 template <int E>
@@ -1425,12 +1468,12 @@ void xpbd_mat(int mat, const SceneDev* scenes, const int* elems, int begin, int 
     constexpr int GPB = kBlock / XpbdLanes<E>::G;
     const int grid = (count + GPB - 1) / GPB;
     switch (mat) {
-        case 0: k_xpbd<E, 0, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
-        case 1: k_xpbd<E, 1, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
-        case 2: k_xpbd<E, 2, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
-        case 3: k_xpbd<E, 3, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
-        case 4: k_xpbd<E, 4, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
-        default: k_xpbd<E, 5, RAW><<<grid, kBlock, 0, st>>>(scenes, elems, begin, count, scene, P); break;
+        case 0: launch_pdl(k_xpbd<E, 0, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
+        case 1: launch_pdl(k_xpbd<E, 1, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
+        case 2: launch_pdl(k_xpbd<E, 2, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
+        case 3: launch_pdl(k_xpbd<E, 3, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
+        case 4: launch_pdl(k_xpbd<E, 4, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
+        default: launch_pdl(k_xpbd<E, 5, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
     }
 }
 template <int E>
@@ -1529,24 +1572,24 @@ void launch_vertex(int element, int material, const SceneDev* scenes, const VWor
 
 void launch_commit(const SceneDev* scenes, const VWork* work, int n_work, cudaStream_t st) {
     if (n_work <= 0) return;
-    k_commit<<<n_work, kBlock, 0, st>>>(scenes, work, n_work);
+    launch_pdl(k_commit, n_work, kBlock, 0, st, scenes, work, n_work);
 }
 
 void launch_predict(const SceneDev* scenes, const NWork* work, int n_work, int kind, int use_force, int chebyshev,
                     const StepParams& P, cudaStream_t st) {
     if (n_work <= 0) return;
-    k_predict<<<n_work, kNodeChunk, 0, st>>>(scenes, work, n_work, kind, use_force, chebyshev, P);
+    launch_pdl(k_predict, n_work, kNodeChunk, 0, st, scenes, work, n_work, kind, use_force, chebyshev, P);
 }
 
 void launch_velocity(const SceneDev* scenes, const NWork* work, int n_work, float global_damping, int pbd,
                      const StepParams& P, cudaStream_t st) {
     if (n_work <= 0) return;
-    k_velocity<<<n_work, kNodeChunk, 0, st>>>(scenes, work, n_work, global_damping, pbd, P);
+    launch_pdl(k_velocity, n_work, kNodeChunk, 0, st, scenes, work, n_work, global_damping, pbd, P);
 }
 
 void launch_chebyshev(const SceneDev* scenes, const NWork* work, int n_work, const StepParams& P, cudaStream_t st) {
     if (n_work <= 0) return;
-    k_chebyshev<<<n_work, kNodeChunk, 0, st>>>(scenes, work, n_work, P);
+    launch_pdl(k_chebyshev, n_work, kNodeChunk, 0, st, scenes, work, n_work, P);
 }
 
 void launch_effect(const SceneDev* scene, const NWork* work, int n_work, int slot, int kind, float dt, cudaStream_t st) {
@@ -1565,7 +1608,7 @@ void launch_wait_probe(int* error, long limit, cudaStream_t st) { k_wait_probe<<
 
 void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, int box_pass, cudaStream_t st) {
     if (n_work <= 0) return;
-    k_constraints<<<n_work, kNodeChunk, 0, st>>>(scenes, work, n_work, box_pass);
+    launch_pdl(k_constraints, n_work, kNodeChunk, 0, st, scenes, work, n_work, box_pass);
 }
 
 void launch_xpbd(int element, int material, bool raw, const SceneDev* scenes, const int* elems, int begin, int count,
