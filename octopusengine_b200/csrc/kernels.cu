@@ -898,6 +898,28 @@ __global__ void k_mg_prolong(const SceneDev* __restrict__ main, const int* __res
 // Failure-detection probe: one thread waits, through the same bounded mbarrier wait as the
 // colour kernels, on a phase that no copy and no thread will ever complete; when the limit
 // runs out it records the time-out in the context's error word (bit 0) and returns.
+__global__ void k_nodes_out(const float4* __restrict__ src, const float4* __restrict__ X, float* __restrict__ out, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 a = src[i];
+    if (X) {
+        const float4 x = X[i];
+        a.x = x.x + a.x; a.y = x.y + a.y; a.z = x.z + a.z;
+    }
+    out[3 * i] = a.x; out[3 * i + 1] = a.y; out[3 * i + 2] = a.z;
+}
+
+__global__ void k_nodes_in(const float* __restrict__ in, const float4* __restrict__ X, float4* __restrict__ dst, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float a = in[3 * i], b = in[3 * i + 1], c = in[3 * i + 2];
+    if (X) {
+        const float4 x = X[i];
+        a = a - x.x; b = b - x.y; c = c - x.z;
+    }
+    dst[i] = make_float4(a, b, c, 0.f);
+}
+
 __global__ void k_wait_probe(int* error, long limit) {
     __shared__ __align__(8) unsigned long long bar;
     const unsigned mb = (unsigned)__cvta_generic_to_shared(&bar);
@@ -1605,6 +1627,12 @@ void launch_mg_prolong(const SceneDev* main, const int* list, int count, int k, 
 }
 
 void launch_wait_probe(int* error, long limit, cudaStream_t st) { k_wait_probe<<<1, 1, 0, st>>>(error, limit); }
+void launch_nodes_out(const float4* src, const float4* X, float* out, int n, cudaStream_t st) {
+    if (n > 0) k_nodes_out<<<(n + 255) / 256, 256, 0, st>>>(src, X, out, n);
+}
+void launch_nodes_in(const float* in, const float4* X, float4* dst, int n, cudaStream_t st) {
+    if (n > 0) k_nodes_in<<<(n + 255) / 256, 256, 0, st>>>(in, X, dst, n);
+}
 
 void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, int box_pass, cudaStream_t st) {
     if (n_work <= 0) return;

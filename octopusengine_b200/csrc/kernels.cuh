@@ -27,6 +27,10 @@ void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, i
 // and the prolongation of mid nodes from k corners with weight w.
 void launch_mg_copy(const SceneDev* main, const SceneDev* sub, const int* map, int n, int dir, cudaStream_t st);
 void launch_mg_prolong(const SceneDev* main, const int* list, int count, int k, float w, cudaStream_t st);
+// Node state as the reference's n x 3 float arrays: out = src (+ X when X is given) and
+// dst = in (- X when X is given), w = 0.
+void launch_nodes_out(const float4* src, const float4* X, float* out, int n, cudaStream_t st);
+void launch_nodes_in(const float* in, const float4* X, float4* dst, int n, cudaStream_t st);
 // Failure-detection probe: a bounded wait on a phase nothing completes (error bit 0 on time-out).
 void launch_wait_probe(int* error, long limit, cudaStream_t st);
 // One scripted effect of one scene (kind 0 crush / 1 random sphere over the node chunks in

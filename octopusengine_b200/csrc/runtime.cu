@@ -173,6 +173,7 @@ struct oct_scene {
     int* d_elems = nullptr;         // XPBD: colour-sorted element ids
     std::vector<int> elem_off;
     double* d_red = nullptr;        // 4 doubles of reduction scratch
+    float* d_io = nullptr;          // n_nodes x 3 floats: node state in and out (allocated on first use)
     float* d_diag = nullptr;        // per-element diagnostics output (allocated on first use)
     // scripted effects (oct_scene_add_effect): host copy of the device slots
     EffectDev effects[kMaxEffects];
@@ -845,18 +846,27 @@ void explicit_substep(oct_scene* s, float dt) {
     if (s->box) { launch_constraints(s->d_scene, s->d_nwork, s->n_nwork, 1, st); c->launches++; }
 }
 
+// Node state out: converted to n x 3 floats on the device and read back in one copy (the
+// caller's buffer may be pinned or pageable); returns when `out` holds the values.
 oct_status read_nodes(oct_scene* s, const float4* d, float* out, bool add_rest) {
     oct_ctx* c = s->ctx;
-    std::vector<float4> h(s->n_nodes);
+    oct_status st;
+    if (!s->d_io && (st = s->mem.alloc(s->d_io, (size_t)s->n_nodes * 3))) return st;
+    launch_nodes_out(d, add_rest ? s->h.X : nullptr, s->d_io, s->n_nodes, c->stream);
+    OCT_CUDA(c, cudaMemcpyAsync(out, s->d_io, sizeof(float) * 3 * s->n_nodes, cudaMemcpyDeviceToHost, c->stream));
     OCT_CUDA(c, cudaStreamSynchronize(c->stream));
-    OCT_CUDA(c, cudaMemcpy(h.data(), d, sizeof(float4) * s->n_nodes, cudaMemcpyDeviceToHost));
-    for (int i = 0; i < s->n_nodes; ++i) {
-        if (add_rest) {
-            out[3 * i] = s->X[3 * i] + h[i].x; out[3 * i + 1] = s->X[3 * i + 1] + h[i].y; out[3 * i + 2] = s->X[3 * i + 2] + h[i].z;
-        } else {
-            out[3 * i] = h[i].x; out[3 * i + 1] = h[i].y; out[3 * i + 2] = h[i].z;
-        }
-    }
+    return OCT_OK;
+}
+
+// Node state in: one copy of the caller's n x 3 floats, converted on the device; returns when
+// the caller may reuse `in`.
+oct_status write_nodes(oct_scene* s, const float* in, float4* d, bool sub_rest) {
+    oct_ctx* c = s->ctx;
+    oct_status st;
+    if (!s->d_io && (st = s->mem.alloc(s->d_io, (size_t)s->n_nodes * 3))) return st;
+    OCT_CUDA(c, cudaMemcpyAsync(s->d_io, in, sizeof(float) * 3 * s->n_nodes, cudaMemcpyHostToDevice, c->stream));
+    launch_nodes_in(s->d_io, sub_rest ? s->h.X : nullptr, d, s->n_nodes, c->stream);
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
     return OCT_OK;
 }
 
@@ -1045,20 +1055,11 @@ oct_status oct_scene_get_velocities(oct_scene* s, float* out) {
 }
 oct_status oct_scene_set_positions(oct_scene* s, const float* in) {
     if (!s || !in) return OCT_EINVAL;
-    std::vector<float4> h(s->n_nodes);
-    for (int i = 0; i < s->n_nodes; ++i)
-        h[i] = make_float4(in[3 * i] - s->X[3 * i], in[3 * i + 1] - s->X[3 * i + 1], in[3 * i + 2] - s->X[3 * i + 2], 0.f);
-    OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
-    OCT_CUDA(s->ctx, cudaMemcpy(s->h.u, h.data(), sizeof(float4) * s->n_nodes, cudaMemcpyHostToDevice));
-    return OCT_OK;
+    return write_nodes(s, in, s->h.u, true);
 }
 oct_status oct_scene_set_velocities(oct_scene* s, const float* in) {
     if (!s || !in) return OCT_EINVAL;
-    std::vector<float4> h(s->n_nodes);
-    for (int i = 0; i < s->n_nodes; ++i) h[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 0.f);
-    OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
-    OCT_CUDA(s->ctx, cudaMemcpy(s->h.v, h.data(), sizeof(float4) * s->n_nodes, cudaMemcpyHostToDevice));
-    return OCT_OK;
+    return write_nodes(s, in, s->h.v, false);
 }
 
 oct_status oct_scene_info(oct_scene* s, int32_t* nn, int32_t* ne, int32_t* nc, int32_t* nf) {
