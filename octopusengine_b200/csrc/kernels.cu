@@ -510,7 +510,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned mb, unsigned phase, long limi
 // the next item's entries arrive while the current item computes, leaving the node-
 // displacement gathers as the only dependent global loads.
 // Resident blocks per SM each element type is compiled for (register cap without spills).
-template <int E> struct MinBlocks { static constexpr int value = E == 3 ? 8 : (E == 7 ? 5 : (E == 6 ? 4 : (E == 8 ? 3 : 2))); };
+template <int E> struct MinBlocks { static constexpr int value = E == 3 ? 8 : (E == 7 ? 5 : (E == 6 ? 4 : (E == 8 ? 4 : 2))); };
 
 template <int E, int MAT>
 __global__ void __launch_bounds__(kBlock, MinBlocks<E>::value) k_vertex_packed(const SceneDev* __restrict__ scenes,
