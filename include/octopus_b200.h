@@ -142,6 +142,12 @@ oct_status oct_scene_set_capture(oct_scene* s, int on);
 /* GPU_ParticleSystem::get_position / get_velocity (synchronous D2H into host arrays). */
 oct_status oct_scene_get_positions(oct_scene* s, float* out_n3);
 oct_status oct_scene_get_velocities(oct_scene* s, float* out_n3);
+/* Node state in (new: the reference has getters only).  VBD moves by the implicit velocity
+ * (p - last_p) / dt (GPU_VBD.cu:6-18), so on a VBD scene the velocities set here become that
+ * implicit velocity at the scene's next own sub-step, as oct_scene_desc.initial_velocity does
+ * (a batch takes the flag when it is created); positions set alone keep the previous
+ * last_p.  Setting positions and then zero velocities restarts a VBD scene at rest in the
+ * given configuration. */
 oct_status oct_scene_set_positions(oct_scene* s, const float* in_n3);
 oct_status oct_scene_set_velocities(oct_scene* s, const float* in_n3);
 oct_status oct_scene_info(oct_scene* s, int32_t* n_nodes, int32_t* n_elements, int32_t* n_colors, int32_t* n_fixed);
@@ -208,14 +214,24 @@ oct_status oct_scene_residual(oct_scene* s, float dt, double out2[2]);
  *   OCT_DIAG_VOLUME_DIFF sum_q (|det Jx_q| w_q - V_q)   (the reference getter launches the
  *                        inversion kernel instead; octb::GPU_FEM::get_volume_diff does the same)
  *   OCT_DIAG_INVERTED    1 where sum_q det(F_q) w_q < -1e-6, else 0
+ *   OCT_DIAG_VOLUME_ACCUMULATED       sum_q |det(sum_{q' <= q} Jx_q')| w_q: the volume with the
+ *                        stress kernel's accumulation, the form of the "volume" field in the
+ *                        reference's result files (assets/result/vtk/References/*.vtk)
+ *   OCT_DIAG_VOLUME_DIFF_ACCUMULATED  the same minus sum_q V_q (their "volume_diff" field)
  * Corotated and FixedCorotated have no stress (0), as in the reference. */
 enum { OCT_DIAG_STRESS = 0, OCT_DIAG_VOLUME = 1, OCT_DIAG_VOLUME_DIFF = 2, OCT_DIAG_INVERTED = 3,
-       OCT_DIAG_STRESS_ACCUMULATED = 4 };
+       OCT_DIAG_STRESS_ACCUMULATED = 4, OCT_DIAG_VOLUME_ACCUMULATED = 5, OCT_DIAG_VOLUME_DIFF_ACCUMULATED = 6 };
 oct_status oct_scene_element_data(oct_scene* s, int kind, float* out_n_elements);
 /* Per-vertex residual force of GPU_VBD_FEM::get_forces (octopus/src/GPU/VBD/GPU_VBD_FEM.cu:
  * 482-559) for sub-step dt: elastic + damping + inertia terms, 0 on fixed vertices; zeros for
  * XPBD and explicit scenes (GPU_FEM::get_forces).  out: n_nodes*3. */
 oct_status oct_scene_vertex_residuals(oct_scene* s, float dt, float* out_n3);
+/* Failure state of a scene's own steps (new: the reference checks nothing).  Waits for the
+ * context stream, then reads and clears the flags the scene's kernels raised since the last
+ * query: OCT_ENUMERIC when a node's position or velocity became NaN / Inf in a sub-step,
+ * OCT_ETIMEDOUT when a bounded device wait gave up (the rest of that colour sweep was left
+ * unsolved), else the context's own error word (OCT_OK when clear). */
+oct_status oct_scene_status(oct_scene* s);
 
 /* Batch: many VBD scenes stepped together, one launch per (element type, colour) across all
  * scenes, driven by a per-scene work table, the sub-step captured as a CUDA graph.  All
@@ -236,6 +252,12 @@ oct_status oct_scene_get_mapping(oct_scene* s, int32_t* threads_per_vertex);
 oct_status oct_autotune_mapping(oct_ctx* ctx, oct_scene* const* scenes, int n, float dt, int sweeps, int32_t chosen[10]);
 oct_status oct_batch_create(oct_ctx* ctx, oct_scene* const* scenes, int n, oct_batch** out);
 oct_status oct_batch_step(oct_batch* b, float frame_dt, int substeps);
+/* Failure state of every scene during the batch's frames, in one read: out[i] (n scenes, in
+ * the order given to oct_batch_create) is OCT_OK, OCT_ENUMERIC or OCT_ETIMEDOUT as for
+ * oct_scene_status; a time-out that belongs to no single scene (a kernel's constant-table
+ * staging) is reported for all.  Waits for the context stream; reading clears the flags.
+ * Scenes are independent, so one scene's failure leaves the others' results intact. */
+oct_status oct_batch_status(oct_batch* b, int32_t* out_n_scenes);
 /* Captures the sub-step graph for (frame_dt, substeps) without launching it, so that a later
  * oct_batch_step starts at once (the serving loop prepares the next batch this way while the
  * current frame runs). */
@@ -292,6 +314,7 @@ typedef struct oct_server_stats {
     double busy_ms;                                   /* summed device time of the frames */
     size_t bytes_in_use;
     double gap_ms;      /* device idle time between consecutive frames of a busy period */
+    int64_t failed;     /* requests ended by OCT_ENUMERIC / OCT_ETIMEDOUT (oct_server_poll says which) */
 } oct_server_stats;
 
 oct_status oct_server_create(oct_ctx* ctx, const oct_server_config* cfg, oct_server** out);
@@ -301,7 +324,10 @@ oct_status oct_server_submit(oct_server* srv, const oct_scene_desc* desc, int32_
 /* One scheduling round: start admissions that fit, run one batched frame of the active
  * scenes, retire finished requests.  Returns the number of active scenes after the frame. */
 oct_status oct_server_tick(oct_server* srv, int32_t* n_active);
-/* done = 1 when the request has finished; then positions (n_nodes*3, may be NULL) are copied out. */
+/* done = 1 when the request has finished; then positions (n_nodes*3, may be NULL) are copied out.
+ * After every frame the server reads the per-scene failure state (oct_batch_status): a request
+ * whose state went NaN / Inf or whose work timed out leaves at once, done = 1, and poll returns
+ * OCT_ENUMERIC or OCT_ETIMEDOUT for it (no positions); the other requests go on unchanged. */
 oct_status oct_server_poll(oct_server* srv, int64_t request_id, int32_t* done, float* positions);
 oct_status oct_server_get_stats(oct_server* srv, oct_server_stats* out);
 oct_status oct_server_destroy(oct_server* srv);

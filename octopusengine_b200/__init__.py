@@ -19,7 +19,9 @@ import ctypes as C
 import numpy as np
 
 from . import capi
-from .capi import (COLOR_DSAT, COLOR_GREEDY, COROTATED, ELEMENT_NODES, FIXED_COROTATED, HEXA, HEXA27, HOOKE,
+from .capi import (COLOR_DSAT, COLOR_GREEDY, COROTATED, DIAG_INVERTED, DIAG_STRESS, DIAG_STRESS_ACCUMULATED,
+                   DIAG_VOLUME, DIAG_VOLUME_ACCUMULATED, DIAG_VOLUME_DIFF, DIAG_VOLUME_DIFF_ACCUMULATED,
+                   ELEMENT_NODES, FIXED_COROTATED, HEXA, HEXA27, HOOKE,
                    MASS_FEMSHAPE, MASS_UNIFORM, NEOHOOKE, ORDER_ASCENDING, ORDER_SHUFFLED, PREC_MIXED, PREC_PLAIN,
                    SOLVER_EXPLICIT, SOLVER_VBD, SOLVER_XPBD, STABLE_NEOHOOKE, STVK, TETRA, TETRA10, TETRA20, VBD_BASE,
                    VBD_BETTER_COLORATION, VBD_REDUCTION_SYMMETRY, XPBD_OPTIGROUP, XPBD_OPTISHARED, XPBD_QUADRATURE,
@@ -247,6 +249,10 @@ class Scene:
         capi.check(capi.lib().oct_scene_get_topology(self._h, capi.ptr(out, C.c_int32)), "oct_scene_get_topology")
         return out
 
+    def status(self):
+        """Failure state of the scene's own steps (oct_scene_status): the oct_status value."""
+        return capi.lib().oct_scene_status(self._h)
+
     def element_data(self, kind):
         """Per-element diagnostic (capi.DIAG_STRESS / VOLUME / VOLUME_DIFF / INVERTED)."""
         out = np.zeros(self.n_elements, np.float32)
@@ -301,6 +307,13 @@ class Batch:
 
     def step(self, frame_dt, substeps=1):
         capi.check(capi.lib().oct_batch_step(self._h, frame_dt, substeps), "oct_batch_step", self.ctx.handle)
+
+    def status(self):
+        """Per-scene failure state of the batch's frames (oct_batch_status), read and cleared."""
+        out = np.zeros(len(self.scenes), np.int32)
+        capi.check(capi.lib().oct_batch_status(self._h, capi.ptr(out, C.c_int32)), "oct_batch_status",
+                   self.ctx.handle)
+        return out
 
     def set_state(self, host):
         capi.check(capi.lib().oct_batch_set_state(self._h, capi.ptr(host, C.c_float)), "oct_batch_set_state")

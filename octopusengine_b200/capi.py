@@ -20,6 +20,7 @@ ELEMENT_QUADRATURE = {TETRA: 1, HEXA: 8, TETRA10: 4, TETRA20: 11, HEXA27: 27}
 HOOKE, STVK, NEOHOOKE, STABLE_NEOHOOKE, COROTATED, FIXED_COROTATED = 0, 1, 2, 3, 4, 5
 XPBD_XPBD, XPBD_QUADRATURE, XPBD_OPTISHARED, XPBD_OPTIGROUP = 0, 1, 2, 3
 DIAG_STRESS, DIAG_VOLUME, DIAG_VOLUME_DIFF, DIAG_INVERTED, DIAG_STRESS_ACCUMULATED = 0, 1, 2, 3, 4
+DIAG_VOLUME_ACCUMULATED, DIAG_VOLUME_DIFF_ACCUMULATED = 5, 6
 EFFECT_CRUSH, EFFECT_RANDOM_SPHERE, EFFECT_HIGH_STRETCH = 0, 1, 2
 MASS_UNIFORM, MASS_FEMSHAPE = 0, 1
 SOLVER_VBD, SOLVER_XPBD, SOLVER_EXPLICIT = 0, 1, 2
@@ -47,6 +48,7 @@ EXPORTS = [
     "oct_beam_sampler_error", "oct_beam_sampler_destroy", "oct_flexion_error", "oct_torsion_profile",
     "oct_scene_add_effect", "oct_scene_set_effect_active", "oct_scene_effect_ids", "oct_surface_nodes",
     "oct_scene_state_size", "oct_scene_save", "oct_scene_restore", "oct_ctx_wait_probe",
+    "oct_scene_status", "oct_batch_status",
 ]
 
 
@@ -68,7 +70,7 @@ class ServerStats(C.Structure):
                 ("rejected", C.c_int64), ("queued", C.c_int64), ("active", C.c_int64), ("frames", C.c_int64),
                 ("p50_step_ms", C.c_double), ("p99_step_ms", C.c_double), ("mean_step_ms", C.c_double),
                 ("vertex_iterations", C.c_double), ("busy_ms", C.c_double), ("bytes_in_use", C.c_size_t),
-                ("gap_ms", C.c_double)]
+                ("gap_ms", C.c_double), ("failed", C.c_int64)]
 
 
 class SceneDesc(C.Structure):
@@ -170,6 +172,8 @@ def lib():
             "oct_batch_create": ([vp, pp, C.c_int, pp], C.c_int),
             "oct_batch_step": ([vp, C.c_float, C.c_int], C.c_int),
             "oct_batch_destroy": ([vp], C.c_int),
+            "oct_scene_status": ([vp], C.c_int),
+            "oct_batch_status": ([vp, ip], C.c_int),
             "oct_batch_set_state": ([vp, fp], C.c_int),
             "oct_batch_get_state": ([vp, fp], C.c_int),
             "oct_batch_state_size": ([vp, C.POINTER(C.c_size_t)], C.c_int),

@@ -75,7 +75,12 @@ struct SceneDev {
     int box_limit;
     int precision;                     // 0 plain, 1 mixed
     EffectDev* effects;                // kMaxEffects slots (scene memory)
+    int* status;                       // per-scene failure flags: kStatusTimeout, kStatusNonFinite
 };
+
+// Per-scene failure flags (SceneDev::status), read and cleared by the host after a frame.
+constexpr int kStatusTimeout = 1;      // a bounded wait gave up on this scene's work
+constexpr int kStatusNonFinite = 2;    // a node's position or velocity became NaN / Inf
 
 // One unit of colour work: `count` consecutive colour slots of one scene.  With a fixed
 // number of lanes per vertex an item fills one block (128 / lanes slots); in the packed

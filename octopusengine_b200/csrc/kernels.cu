@@ -107,8 +107,13 @@ __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;"
 
 // ------------------------------------------------------------------------ TMA staging
 // One elected thread issues a cp.async.bulk global->shared copy tracked by an mbarrier;
-// every thread waits on the barrier with an iteration limit.  On time-out the kernel
-// records an error and falls back to plain loads, so a wait can never hang the GPU.
+// every thread waits on the barrier with an iteration limit.  The phase completes once for
+// the whole block, so one thread seeing it complete means the copy has landed; the block
+// decides together (__syncthreads_or) whether any thread saw it.  If none did, the kernel
+// records a time-out, gives the copy in flight a second bounded wait (so it does not land
+// after the fallback or after the block has left), then loads the table with plain loads:
+// a wait can never hang the GPU and every thread reaches the same barriers.
+__device__ __forceinline__ bool mbar_wait(unsigned mb, unsigned phase, long limit);
 __device__ __forceinline__ void stage_table(float* s_dst, const float* g_src, int n_floats, unsigned long long* mbar,
                                             int* error) {
     const int bytes = ((n_floats * 4 + 15) / 16) * 16;
@@ -124,13 +129,10 @@ __device__ __forceinline__ void stage_table(float* s_dst, const float* g_src, in
         asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                      ::"r"(dst), "l"(g_src), "r"(bytes), "r"(mb) : "memory");
     }
-    unsigned done = 0;
-    for (long it = 0; it < kSpinLimit && !done; ++it) {
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
-                     : "=r"(done) : "r"(mb) : "memory");
-    }
-    if (!done) {
-        if (error) atomicOr(error, 1);
+    const bool done = mbar_wait(mb, 0, kSpinLimit);
+    if (!__syncthreads_or(done)) {   // block-uniform: nobody saw the copy land
+        if (threadIdx.x == 0 && error) atomicOr(error, 1);
+        mbar_wait(mb, 0, kSpinLimit);
         __syncthreads();
         for (int i = threadIdx.x; i < n_floats; i += blockDim.x) s_dst[i] = g_src[i];
     }
@@ -493,7 +495,7 @@ __device__ __forceinline__ void vertex_epilogue(const SceneDev& S, int vid, cons
 }
 
 // Bounded wait on an mbarrier phase; false when the iteration limit ran out.
-__device__ __forceinline__ bool mbar_wait(unsigned mb, unsigned phase, long limit = kSpinLimit) {
+__device__ __forceinline__ bool mbar_wait(unsigned mb, unsigned phase, long limit) {
     unsigned done = 0;
     for (long it = 0; it < limit && !done; ++it)
         asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -552,20 +554,19 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<E>::value) k_vertex_packed(c
     if (lane == 0 && w < n_work) issue(w, 0);   // work items and entries are static: before the wait
     pdl_wait();
     unsigned phase0 = 0, phase1 = 0;
+    int drain = 0;   // after a time-out: 1 + the buffer whose copy timed out (+2 if the other is in flight)
     for (int k = 0; w < n_work; ++k, w += stride) {
         const int b = k & 1;
         if (lane == 0 && w + stride < n_work) issue(w + stride, b ^ 1);
         const VWork wk = work[w];
         const SceneDev& S = scenes[wk.scene];
         float* buf = b ? buf1 : buf0;
-        const bool ok = mbar_wait(b ? bar1 : bar0, b ? phase1 : phase0);
-        if (b) phase1 ^= 1; else phase0 ^= 1;
-        if (!__all_sync(full, ok)) {   // time-out: record it and load this item directly
-            if (lane == 0) atomicOr(P.error, 1);
-            if (lane < wk.n_pairs)
-                for (int j = 0; j < EW; ++j) buf[lane * EW + j] = reinterpret_cast<const float*>(S.ent)[((size_t)wk.pair_base + lane) * EW + j];
-            __syncwarp();
+        const bool ok = mbar_wait(b ? bar1 : bar0, b ? phase1 : phase0, kSpinLimit);
+        if (!__all_sync(full, ok)) {   // time-out (warp-uniform): leave the loop, handled below
+            drain = 1 + b + (w + stride < n_work ? 2 : 0);
+            break;
         }
+        if (b) phase1 ^= 1; else phase0 ^= 1;
         const float* en = buf + lane * EW;
         const unsigned upto = wk.heads & ((2u << lane) - 1u);
         const int head = 31 - __clz(upto);
@@ -599,6 +600,17 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<E>::value) k_vertex_packed(c
         }
         if (active && lane == head) vertex_epilogue(S, vid, acc, mode, P, red);
         __syncwarp();   // buffer b is refilled by the next-but-one issue
+    }
+    if (drain) {
+        // record the time-out (the warp's remaining items are not solved; the host reports
+        // OCT_ETIMEDOUT), then give the timed-out copy, and the one issued into the other
+        // buffer, a second bounded wait, so neither lands in shared memory after this warp
+        // has stopped tracking it
+        if (lane == 0) { atomicOr(P.error, 1); atomicOr(scenes[work[w].scene].status, kStatusTimeout); }
+        const int b = (drain - 1) & 1;
+        mbar_wait(b ? bar1 : bar0, b ? phase1 : phase0, kSpinLimit);
+        if (drain > 2) mbar_wait(b ? bar0 : bar1, b ? phase0 : phase1, kSpinLimit);
+        __syncwarp();
     }
     pdl_trigger();   // after the sweep: the next launch overlaps this kernel's tail only
 }
@@ -720,6 +732,7 @@ __global__ void k_predict(const SceneDev* __restrict__ scenes, const NWork* __re
         u.x += v.x * dt; u.y += v.y * dt; u.z += v.z * dt;
         S.v[i] = v;
         S.u[i] = u;
+        if (!isfinite(u.x + u.y + u.z + v.x + v.y + v.z)) atomicOr(S.status, kStatusNonFinite);
     }
 }
 
@@ -743,6 +756,8 @@ __global__ void k_velocity(const SceneDev* __restrict__ scenes, const NWork* __r
         }
     }
     S.v[i] = v;
+    // end of the sub-step: one check per node flags a scene whose state blew up
+    if (!isfinite(u.x + u.y + u.z + v.x + v.y + v.z)) atomicOr(S.status, kStatusNonFinite);
 }
 
 // Chebyshev semi-iterative acceleration (kernel_chebychev_acceleration, GPU_VBD.cu:27-36).
@@ -1288,7 +1303,7 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const SceneDev* __restr
     const double* wt = gwd<E>();
     const float4 c0 = S.eq[(size_t)eid * S.eq_stride * 3 + 2];   // lambda, mu of the element
     const double lam = c0.z, mu = c0.w;
-    D3 A0 = {0, 0, 0}, A1 = A0, A2 = A0;   // accumulated Jx (kind 4)
+    D3 A0 = {0, 0, 0}, A1 = A0, A2 = A0;   // accumulated Jx (kinds 4, 5, 6)
     double acc = 0.0;
     for (int q = 0; q < NQ; ++q) {
         D3 J0 = {0, 0, 0}, J1 = J0, J2 = J0, R0 = J0, R1 = J0, R2 = J0;
@@ -1305,6 +1320,11 @@ __global__ void __launch_bounds__(kBlock) k_element_diag(const SceneDev* __restr
         const double Vq = fabs(ddet(R0, R1, R2)) * w;
         if (kind == 1) { acc += fabs(ddet(J0, J1, J2)) * w; continue; }
         if (kind == 2) { acc += fabs(ddet(J0, J1, J2)) * w - Vq; continue; }
+        if (kind == 5 || kind == 6) {
+            A0 = A0 + J0; A1 = A1 + J1; A2 = A2 + J2;
+            acc += fabs(ddet(A0, A1, A2)) * w - (kind == 6 ? Vq : 0.0);
+            continue;
+        }
         D3 m0, m1, m2;   // JX_inv columns
         dinv(R0, R1, R2, m0, m1, m2);
         if (kind == 4) { A0 = A0 + J0; A1 = A1 + J1; A2 = A2 + J2; J0 = A0; J1 = A1; J2 = A2; }

@@ -164,6 +164,7 @@ struct oct_scene {
     SceneDev* d_scene = nullptr;
     int* d_pending = nullptr;
     int pending_host = 0;
+    int* d_status = nullptr;        // SceneDev::status of the scene's own steps
     VWork* d_vwork = nullptr;
     std::vector<int> vwork_off;     // per colour: [vwork_off[c], vwork_off[c+1])
     NWork* d_nwork = nullptr;
@@ -197,6 +198,7 @@ struct oct_batch {
     SceneDev* d_scenes = nullptr;
     int* d_pending = nullptr;
     std::vector<int> pending_host;
+    int* d_status = nullptr;        // SceneDev::status of each scene during the batch's frames
     struct Group {
         int element, material, tpv;
         bool in_place;
@@ -693,6 +695,8 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     for (int k = 0; k < kMaxEffects; ++k) { s->effects[k] = EffectDev{}; s->effects[k].kind = -1; }
     if ((st = upload(c, s->mem, s->d_effects, std::vector<EffectDev>(s->effects, s->effects + kMaxEffects)))) return st;
     h.effects = s->d_effects;
+    if ((st = upload(c, s->mem, s->d_status, std::vector<int>{0}))) return st;
+    h.status = s->d_status;
     s->topo_host.assign(d->topology, d->topology + (size_t)E * NE);
     if ((st = s->mem.alloc(s->d_scene, 1))) return st;
     OCT_CUDA(c, cudaMemcpy(s->d_scene, &h, sizeof(SceneDev), cudaMemcpyHostToDevice));
@@ -1059,7 +1063,13 @@ oct_status oct_scene_set_positions(oct_scene* s, const float* in) {
 }
 oct_status oct_scene_set_velocities(oct_scene* s, const float* in) {
     if (!s || !in) return OCT_EINVAL;
-    return write_nodes(s, in, s->h.v, false);
+    oct_status st = write_nodes(s, in, s->h.v, false);
+    if (st || s->solver != OCT_SOLVER_VBD) return st;
+    // VBD moves by the implicit velocity (p - last_p) / dt; like an initial velocity, the set
+    // velocities become it at the scene's next sub-step (u_last = u - v dt in the predictor)
+    s->pending_host = 1;
+    OCT_CUDA(s->ctx, cudaMemcpy(s->d_pending, &s->pending_host, sizeof(int), cudaMemcpyHostToDevice));
+    return OCT_OK;
 }
 
 oct_status oct_scene_info(oct_scene* s, int32_t* nn, int32_t* ne, int32_t* nc, int32_t* nf) {
@@ -1323,7 +1333,7 @@ oct_status oct_scene_energy(oct_scene* s, double out[4]) {
 }
 
 oct_status oct_scene_element_data(oct_scene* s, int kind, float* out) {
-    if (!s || !out || kind < OCT_DIAG_STRESS || kind > OCT_DIAG_STRESS_ACCUMULATED) return OCT_EINVAL;
+    if (!s || !out || kind < OCT_DIAG_STRESS || kind > OCT_DIAG_VOLUME_DIFF_ACCUMULATED) return OCT_EINVAL;
     oct_ctx* c = s->ctx;
     oct_status st;
     if (!s->d_diag && (st = s->mem.alloc(s->d_diag, (size_t)s->n_elements))) return st;
@@ -1367,6 +1377,34 @@ oct_status oct_scene_residual(oct_scene* s, float dt, double out[2]) {
     OCT_CUDA(c, cudaMemcpyAsync(out, s->d_red, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     OCT_CUDA(c, cudaStreamSynchronize(c->stream));
     return check_error_word(c);
+}
+
+oct_status oct_scene_status(oct_scene* s) {
+    if (!s) return OCT_EINVAL;
+    oct_ctx* c = s->ctx;
+    int f = 0;
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    OCT_CUDA(c, cudaMemcpy(&f, s->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (f) OCT_CUDA(c, cudaMemset(s->d_status, 0, sizeof(int)));
+    if (f & kStatusNonFinite) return fail(c, OCT_ENUMERIC, "non-finite position or velocity in the scene");
+    if (f & kStatusTimeout) return fail(c, OCT_ETIMEDOUT, "a bounded device wait gave up on the scene's work");
+    return check_error_word(c);
+}
+
+oct_status oct_batch_status(oct_batch* b, int32_t* out) {
+    if (!b || !out) return OCT_EINVAL;
+    oct_ctx* c = b->ctx;
+    const size_t n = b->scenes.size();
+    std::vector<int> f(n, 0);
+    OCT_CUDA(c, cudaStreamSynchronize(c->stream));
+    OCT_CUDA(c, cudaMemcpy(f.data(), b->d_status, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    OCT_CUDA(c, cudaMemset(b->d_status, 0, sizeof(int) * n));
+    int e = 0;   // context word: a time-out outside any one scene's work (constant-table staging)
+    OCT_CUDA(c, cudaMemcpy(&e, c->d_error, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e & 1) OCT_CUDA(c, cudaMemset(c->d_error, 0, sizeof(int)));
+    for (size_t i = 0; i < n; ++i)
+        out[i] = (f[i] & kStatusNonFinite) ? OCT_ENUMERIC : ((f[i] & kStatusTimeout) || (e & 1)) ? OCT_ETIMEDOUT : OCT_OK;
+    return OCT_OK;
 }
 
 oct_status oct_ctx_stream(oct_ctx* c, void** stream) {
@@ -1459,6 +1497,9 @@ oct_status oct_batch_create(oct_ctx* c, oct_scene* const* scenes, int n, oct_bat
     }
     OCT_CUDA(c, cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
     oct_status st;
+    // the batch's scene copies report failures into the batch's own status array
+    if ((st = upload(c, b->mem, b->d_status, std::vector<int>(b->scenes.size(), 0)))) { b->mem.release(); return st; }
+    for (size_t i = 0; i < hs.size(); ++i) hs[i].status = b->d_status + i;
     if ((st = upload(c, b->mem, b->d_scenes, hs)) || (st = upload(c, b->mem, b->d_vwork, all)) ||
         (st = upload(c, b->mem, b->d_nwork, nw)) || (st = upload(c, b->mem, b->d_fwork, fw)) ||
         (st = upload(c, b->mem, b->d_bwork, bw)) || (st = upload(c, b->mem, b->d_pending, b->pending_host))) {
@@ -1552,7 +1593,10 @@ oct_status oct_batch_step(oct_batch* b, float frame_dt, int substeps) {
         c->launches += batch_launches_per_substep(b);
     }
     cudaEventRecord(c->ev1, c->stream);
-    for (auto* s : b->scenes) s->pending_host = 0;
+    for (auto* s : b->scenes) {   // the batch applied them; the scenes' own flags go too
+        if (s->pending_host) cudaMemsetAsync(s->d_pending, 0, sizeof(int), c->stream);
+        s->pending_host = 0;
+    }
     return OCT_OK;
 }
 

@@ -60,7 +60,7 @@ struct oct_server {
     bool dirty = true;
     std::vector<double> frame_ms;
     double vertex_iterations = 0, busy_ms = 0;
-    int64_t submitted = 0, admitted = 0, finished = 0, rejected = 0;
+    int64_t submitted = 0, admitted = 0, finished = 0, rejected = 0, failed = 0;
     cudaEvent_t e0 = nullptr, e1 = nullptr, prev_end = nullptr;
     bool have_prev = false;
     double gap_ms = 0;   // device idle time between consecutive frames
@@ -217,6 +217,14 @@ oct_status oct_server_tick(oct_server* s, int32_t* n_active) {
         const bool changed = leaving || !s->joining.empty();
         if (changed && (st = build_batch(s, next, &next_batch))) return st;
         if (cudaEventSynchronize(s->e1) != cudaSuccess) return OCT_ECUDA;
+        // per-request failure state of the frame: a request whose state went non-finite or
+        // whose work timed out ends with that status; scenes are independent, so the others
+        // carry on unchanged
+        std::vector<int32_t> flags(s->active.size(), OCT_OK);
+        if ((st = oct_batch_status(s->batch, flags.data()))) return st;
+        std::vector<Request*> failed;
+        for (size_t i = 0; i < s->active.size(); ++i)
+            if (flags[i] != OCT_OK) { s->active[i]->status = (oct_status)flags[i]; failed.push_back(s->active[i]); }
         float ms = 0.f, gap = 0.f;
         cudaEventElapsedTime(&ms, s->e0, s->e1);
         if (s->have_prev && cudaEventElapsedTime(&gap, s->prev_end, s->e0) == cudaSuccess) s->gap_ms += gap;
@@ -230,19 +238,29 @@ oct_status oct_server_tick(oct_server* s, int32_t* n_active) {
         }
         for (auto* r : s->active) {
             s->vertex_iterations += (double)r->free_nodes * s->cfg.iterations * s->cfg.substeps;
-            if (++r->steps_done >= r->steps_total) {
-                r->result.resize(3 * (size_t)r->desc.n_nodes);
-                r->status = oct_scene_get_positions(r->scene, r->result.data());
+            const bool bad = r->status != OCT_OK;
+            if (++r->steps_done >= r->steps_total || bad) {
+                if (!bad) {
+                    r->result.resize(3 * (size_t)r->desc.n_nodes);
+                    r->status = oct_scene_get_positions(r->scene, r->result.data());
+                }
                 oct_scene_destroy(r->scene);
                 r->scene = nullptr;
                 r->done = true;
                 s->reserved -= r->bytes;
-                s->finished++;
+                if (bad) s->failed++;
+                else s->finished++;
             }
         }
         if (changed) {
             s->active = next;
             s->joining.clear();
+        }
+        if (!failed.empty()) {   // failed requests leave now; the next tick rebuilds the batch
+            auto gone = [&](Request* r) { return std::find(failed.begin(), failed.end(), r) != failed.end(); };
+            s->active.erase(std::remove_if(s->active.begin(), s->active.end(), gone), s->active.end());
+            if (s->batch) { oct_batch_destroy(s->batch); s->batch = nullptr; }
+            s->dirty = true;
         }
     }
     if (s->active.empty()) s->have_prev = false;   // idle: the next gap is not a host delay
@@ -267,6 +285,7 @@ oct_status oct_server_get_stats(oct_server* s, oct_server_stats* o) {
     o->admitted = s->admitted;
     o->finished = s->finished;
     o->rejected = s->rejected;
+    o->failed = s->failed;
     o->queued = (int64_t)s->queue.size();
     o->active = (int64_t)s->active.size();
     o->frames = (int64_t)s->frame_ms.size();

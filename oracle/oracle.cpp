@@ -1039,6 +1039,10 @@ template <class T> void residual_vectors(VBD<T>& b, T dt, double* out) {
 //                   (materials without a VBD stress, Corotated and FixedCorotated, give P = 0)
 //   kind 1 volume   kernel_compute_volume (:45-64): sum_q |det Jx_q| w_q
 //   kind 2 diff     kernel_compute_volume_diff (:66-85): sum_q (|det Jx_q| w_q - V_q)
+//   kind 5 volume   kind 1 with Jx accumulated over the quadrature points as in kind 4, the form
+//                   of the "volume" field of the reference's result files
+//                   (assets/result/vtk/References/*.vtk)
+//   kind 6 diff     kind 2 with the same accumulation (their "volume_diff" field)
 //   kind 3 inverted kernel_compute_inverted (:87-107): 1 when sum_q det(Jx_q JX_inv_q) w_q < -1e-6
 //                   (the kernel indexes JX_inv[eid + qid], outside the element's records and,
 //                   for eid >= E Q / (Q + 1), outside the buffer; the record of q is used here)
@@ -1065,6 +1069,9 @@ template <class T> void element_data(const Fem<T>& f, const State<T>& s, int kin
                 acc += std::fabs(det(Jx)) * f.weights[q];
             } else if (kind == 2) {
                 acc += std::fabs(det(Jx)) * f.weights[q] - Vq;
+            } else if (kind == 5 || kind == 6) {
+                Jacc = Jacc + Jx;
+                acc += std::fabs(det(Jacc)) * f.weights[q] - (kind == 6 ? Vq : T(0));
             } else {
                 acc += det(Jx * Ji) * f.weights[q];
             }
@@ -1391,7 +1398,8 @@ template <class T> int get_state(const State<T>& s, int what, double* out) {
 
 template <class T> int set_state(State<T>& s, int what, const double* in) {
     std::vector<V3<T>>* dst = nullptr;
-    switch (what) { case 0: dst = &s.p; break; case 1: dst = &s.v; break; case 2: dst = &s.last_p; break; default: return -1; }
+    switch (what) { case 0: dst = &s.p; break; case 1: dst = &s.v; break; case 2: dst = &s.last_p; break;
+                 case 3: dst = &s.y; break; default: return -1; }
     for (int i = 0; i < s.n; ++i) for (int k = 0; k < 3; ++k) (*dst)[i][k] = (T)in[3 * i + k];
     return 0;
 }
@@ -1700,7 +1708,7 @@ int orc_vbd_forces(void* hv, float dt, double* out) {
 }
 int orc_element_data(void* hv, int kind, double* out) {
     Handle* h = (Handle*)hv;
-    if (!h || !out || kind < 0 || kind > 4) return -1;
+    if (!h || !out || kind < 0 || kind > 6) return -1;
     switch (h->kind) {
         case 0: element_data(((VBD<float>*)h->ptr)->fem, ((VBD<float>*)h->ptr)->s, kind, out); break;
         case 1: element_data(((VBD<double>*)h->ptr)->fem, ((VBD<double>*)h->ptr)->s, kind, out); break;

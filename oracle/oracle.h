@@ -78,7 +78,7 @@ int orc_conflicts(int element, const int32_t* topology, int n_elements, int n_no
 void* orc_vbd_create(const orc_desc* d, int fp64);
 int orc_vbd_step(void* h, float frame_dt, int substeps);
 int orc_vbd_get(void* h, int what, double* out);   /* what: 0 p, 1 v, 2 last_p, 3 y, 4 mask */
-int orc_vbd_set(void* h, int what, const double* in);
+int orc_vbd_set(void* h, int what, const double* in);  /* what: 0 p, 1 v, 2 last_p, 3 y */
 int orc_vbd_energy(void* h, double* parts);         /* kinetic, elastic, gravity, total */
 int orc_vbd_residual(void* h, float dt, double* out_norms); /* [sum |r|, max |r|] of free nodes */
 /* Per-vertex residual force of kernel_vbd_compute_residual (GPU_VBD_FEM.cu:482-559), n*3;
@@ -88,7 +88,8 @@ void orc_vbd_destroy(void* h);
 
 /* Per-element diagnostics of GPU_FEM (GPU_FEM.cu:20-107) on any solver handle: kind 0 von Mises
  * stress, 1 volume, 2 volume change, 3 inverted flag, 4 von Mises stress with Jx accumulated
- * over the quadrature points (kernel_compute_stress as written); out: n_elements. */
+ * over the quadrature points (kernel_compute_stress as written), 5 volume and 6 volume change
+ * with the same accumulation (the fields of the reference's result files); out: n_elements. */
 int orc_element_data(void* h, int kind, double* out);
 
 /* Rigid motion of fixation group g (GPU_Fix_Constraint axis): p = offset + com + R (X - com),

@@ -29,7 +29,8 @@ import os
 import re
 import sys
 
-REF = "/root/reference"
+# The reference tree; OCTOPUS_REFERENCE overrides the build container's mount point.
+REF = os.environ.get("OCTOPUS_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 

@@ -30,7 +30,7 @@ def test_element_data_matches_oracle(ctx, element, material):
     assert np.abs(p - mesh["X"]).max() > 1e-3   # really deformed
     o64.set(0, p.astype(np.float64))             # the oracle evaluates at the product's positions
     kinds = (ob.capi.DIAG_STRESS, ob.capi.DIAG_VOLUME, ob.capi.DIAG_VOLUME_DIFF, ob.capi.DIAG_INVERTED,
-             ob.capi.DIAG_STRESS_ACCUMULATED)
+             ob.capi.DIAG_STRESS_ACCUMULATED, ob.capi.DIAG_VOLUME_ACCUMULATED, ob.capi.DIAG_VOLUME_DIFF_ACCUMULATED)
     vol = o64.element_data(ob.capi.DIAG_VOLUME)
     for kind in kinds:
         got = s.element_data(kind).astype(np.float64)
@@ -38,14 +38,16 @@ def test_element_data_matches_oracle(ctx, element, material):
         if kind == ob.capi.DIAG_INVERTED:
             np.testing.assert_array_equal(got, ref)
             assert got.sum() == 0
-        elif kind == ob.capi.DIAG_VOLUME_DIFF:
-            assert np.abs(got - ref).max() <= 1e-6 * vol.max()
+        elif kind in (ob.capi.DIAG_VOLUME_DIFF, ob.capi.DIAG_VOLUME_DIFF_ACCUMULATED):
+            assert np.abs(got - ref).max() <= 1e-6 * max(vol.max(), np.abs(ref).max())
         else:
             # both in FP64 at the same positions; the output is rounded to FP32
             assert np.abs(got - ref).max() <= 1e-6 * np.abs(ref).max(), kind
     if element == O.TETRA:   # one quadrature point: nothing to accumulate
         np.testing.assert_array_equal(s.element_data(ob.capi.DIAG_STRESS_ACCUMULATED),
                                       s.element_data(ob.capi.DIAG_STRESS))
+        np.testing.assert_array_equal(s.element_data(ob.capi.DIAG_VOLUME_ACCUMULATED),
+                                      s.element_data(ob.capi.DIAG_VOLUME))
 
 
 def test_volumes_sum_to_the_beam_volume_at_rest(ctx):

@@ -72,3 +72,78 @@ def test_admission_by_hbm_budget(ctx):
     assert ei.value.status == capi.ENOMEM_BUDGET
     assert srv.stats()["rejected"] == 1
     srv.close()
+
+
+def _nan_v0(n):
+    v0 = np.zeros((n, 3), np.float32)
+    v0[n // 2, 1] = np.nan   # a host-side fault: one request's state carries a NaN
+    return v0
+
+
+def test_a_failing_scene_is_reported_alone_in_a_batch(ctx):
+    import octopusengine_b200 as ob
+    from octopusengine_b200 import capi
+    specs = [_spec(i) for i in range(3)]
+    scenes = []
+    for i, (e, X, T, kw) in enumerate(specs):
+        extra = dict(initial_velocity=_nan_v0(len(X))) if i == 1 else {}
+        scenes.append(ob.Scene(ctx, e, X, T, iterations=6, precision=ob.PREC_MIXED, **kw, **extra))
+    b = ob.Batch(ctx, scenes)
+    b.step(1 / 60, 2)
+    np.testing.assert_array_equal(b.status(), [capi.OK, capi.ENUMERIC, capi.OK])
+    np.testing.assert_array_equal(b.status(), [capi.OK] * 3)   # reading cleared the flags
+    for i in (0, 2):
+        e, X, T, kw = specs[i]
+        alone = ob.Scene(ctx, e, X, T, iterations=6, precision=ob.PREC_MIXED, **kw)
+        alone.step(1 / 60, 2)
+        assert alone.status() == capi.OK
+        assert rel_err(scenes[i].get_position(), alone.get_position()) < 1e-6
+        alone.close()
+    b.close()
+    # the same scene stepped alone reports the failure through its own status
+    e, X, T, kw = specs[1]
+    s = ob.Scene(ctx, e, X, T, iterations=6, **kw, initial_velocity=_nan_v0(len(X)))
+    s.step(1 / 60, 1)
+    assert s.status() == capi.ENUMERIC
+    assert s.status() == capi.OK
+    s.close()
+    for sc in scenes:
+        sc.close()
+
+
+def test_a_failed_request_ends_alone_and_the_others_are_unchanged(ctx):
+    import octopusengine_b200 as ob
+    from octopusengine_b200 import capi
+    srv = ob.Server(ctx, frame_dt=1 / 60, substeps=2, iterations=6, precision=ob.PREC_MIXED, max_scenes=64)
+    steps = [4, 6, 5, 3]
+    ids = {}
+    for i in range(len(steps)):
+        e, X, T, kw = _spec(i)
+        ids[i] = srv.submit(e, X, T, steps[i], **kw)
+    e, X, T, kw = _spec(1)
+    bad = srv.submit(e, X, T, 5, initial_velocity=_nan_v0(len(X)), **kw)
+    status = {}
+    for _ in range(40):
+        srv.tick()
+        for i, rid in list(ids.items()) + [("bad", bad)]:
+            if i in status:
+                continue
+            try:
+                if srv.poll(rid, fetch=False) is not None:
+                    status[i] = capi.OK
+            except ob.OctError as err:
+                status[i] = err.status
+        if len(status) == len(steps) + 1:
+            break
+    assert status["bad"] == capi.ENUMERIC
+    assert all(status[i] == capi.OK for i in range(len(steps)))
+    st = srv.stats()
+    assert st["failed"] == 1 and st["finished"] == len(steps)
+    for i, rid in ids.items():
+        e, X, T, kw = _spec(i)
+        alone = ob.Scene(ctx, e, X, T, iterations=6, precision=ob.PREC_MIXED, **kw)
+        for _ in range(steps[i]):
+            alone.step(1 / 60, 2)
+        assert rel_err(srv.poll(rid), alone.get_position()) < 1e-6
+        alone.close()
+    srv.close()
