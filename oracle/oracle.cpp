@@ -848,6 +848,21 @@ template <class T> void mg_prolong(VBD<T>& b) {
     apply(b.pro_vol, 8, T(0.125f));
 }
 
+// Host threads for the vertices of one colour (orc_set_threads).  The vertices of a colour of
+// a conflict-free colouring share no element, so each one reads only other colours' positions
+// and solving them in any order, or at once, gives the same result bit for bit; with conflicts
+// (ColorReduction) the Jacobi path writes p_new and is order-free too.
+static int g_threads = 1;
+template <class F> static void parallel_for(size_t n, F&& body) {
+    const int t = (int)std::min<size_t>((size_t)g_threads, n / 256 + 1);
+    if (t <= 1) { for (size_t i = 0; i < n; ++i) body(i); return; }
+    std::vector<std::thread> pool;
+    const size_t chunk = (n + t - 1) / t;
+    for (int k = 0; k < t; ++k)
+        pool.emplace_back([&, k]() { for (size_t i = k * chunk; i < std::min(n, (k + 1) * chunk); ++i) body(i); });
+    for (auto& th : pool) th.join();
+}
+
 // GPU_VBD::step (GPU_VBD.cu:38-61) + GPU_VBD_FEM::step (GPU_VBD_FEM.cu:712-755) for one
 // sub-step of length dt.
 template <class T> void vbd_substep(VBD<T>& b, T dt) {
@@ -887,19 +902,21 @@ template <class T> void vbd_substep(VBD<T>& b, T dt) {
         for (int c : order) {
             const std::vector<int>& vs = colours[c];
             if (in_place) {
-                for (int vid : vs) {
-                    if (s.mask[vid] == 0) continue;
+                parallel_for(vs.size(), [&](size_t k) {
+                    const int vid = vs[k];
+                    if (s.mask[vid] == 0) return;
                     V3<T> fi; M3<T> H;
                     vbd_vertex(fl, ol, s, vid, dt, fi, H);
                     s.p[vid] = s.p[vid] + vbd_correction(s, vid, b.damping, dt, fi, H, level ? b.m_lin[vid] : T(-1));
-                }
+                });
             } else {
-                for (int vid : vs) {
-                    if (s.mask[vid] == 0) continue;
+                parallel_for(vs.size(), [&](size_t k) {
+                    const int vid = vs[k];
+                    if (s.mask[vid] == 0) return;
                     V3<T> fi; M3<T> H;
                     vbd_vertex(fl, ol, s, vid, dt, fi, H);
                     s.p_new[vid] = s.p[vid] + vbd_correction(s, vid, b.damping, dt, fi, H);
-                }
+                });
                 for (int vid : vs) if (s.mask[vid] != 0) s.p[vid] = s.p_new[vid];   // kernel_copy_in_position
             }
         }
@@ -1683,6 +1700,8 @@ int orc_vbd_get(void* hv, int what, double* out) {
     Handle* h = (Handle*)hv;
     return h->kind == 1 ? get_state(((VBD<double>*)h->ptr)->s, what, out) : get_state(((VBD<float>*)h->ptr)->s, what, out);
 }
+void orc_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+
 int orc_vbd_set(void* hv, int what, const double* in) {
     Handle* h = (Handle*)hv;
     return h->kind == 1 ? set_state(((VBD<double>*)h->ptr)->s, what, in) : set_state(((VBD<float>*)h->ptr)->s, what, in);

@@ -78,6 +78,9 @@ int orc_conflicts(int element, const int32_t* topology, int n_elements, int n_no
 void* orc_vbd_create(const orc_desc* d, int fp64);
 int orc_vbd_step(void* h, float frame_dt, int substeps);
 int orc_vbd_get(void* h, int what, double* out);   /* what: 0 p, 1 v, 2 last_p, 3 y, 4 mask */
+/* Host threads the GPU-semantics VBD sweep may use for the vertices of one colour (default 1;
+ * results are the same bit for bit for any count). */
+void orc_set_threads(int n);
 int orc_vbd_set(void* h, int what, const double* in);  /* what: 0 p, 1 v, 2 last_p, 3 y */
 int orc_vbd_energy(void* h, double* parts);         /* kinetic, elastic, gravity, total */
 int orc_vbd_residual(void* h, float dt, double* out_norms); /* [sum |r|, max |r|] of free nodes */

@@ -72,8 +72,14 @@ def lib():
         L.orc_set_effect_active.argtypes = [vp, C.c_int, C.c_int]
         L.orc_vbd_forces.argtypes = [vp, C.c_float, dp]
         L.orc_xpbd_pair.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, dp, dp, dp]
+        L.orc_set_threads.argtypes = [C.c_int]
         _lib = L
     return _lib
+
+
+def set_threads(n=None):
+    """Host threads for one colour's vertices in the oracle's VBD sweep (None: all cores)."""
+    lib().orc_set_threads(int(n if n is not None else (os.cpu_count() or 1)))
 
 
 def _p(a, t):

@@ -73,9 +73,10 @@ def test_xpbd_element_colouring_matches_reference_order(ctx):
     assert n1 == n2 and np.array_equal(c1, c2)
 
 
-@pytest.mark.parametrize("element", [O.TETRA, O.HEXA, O.TETRA10])
+@pytest.mark.parametrize("element", [O.TETRA, O.HEXA, O.TETRA10, O.TETRA20, O.HEXA27])
 def test_explicit_parity(ctx, element):
-    s, o32, o64, mesh = pair(ctx, element, cells=(4, 2, 2), solver="explicit", young=1e5, damping=1e-4)
+    cells = (3, 2, 2) if element in (O.TETRA20, O.HEXA27) else (4, 2, 2)
+    s, o32, o64, mesh = pair(ctx, element, cells=cells, solver="explicit", young=1e5, damping=1e-4)
     for _ in range(5):
         s.step(1e-3, 20)
         o32.step(1e-3, 20)
