@@ -653,6 +653,8 @@ def main():
     ap.add_argument("--tpv", type=int, default=0, help="lanes per vertex (0 = measured default, -1 = packed pair-per-lane mapping)")
     ap.add_argument("--tpv-elem", default="", help="per-element lanes per vertex, e.g. 3:4,7:-1")
     ap.add_argument("--no-autotune", action="store_true", help="keep the measured default mapping")
+    ap.add_argument("--scenes", type=int, default=0,
+                    help="batched: only the first N scenes of the draw (a smaller case for profiling)")
     ap.add_argument("--no-extra", action="store_true",
                     help="batched: skip the single-scene config-2 figure and the short served stream")
     ap.add_argument("--serve-rate", type=float, default=4.0, help="batched: rate of the short served stream")
@@ -676,6 +678,8 @@ def main():
         bench_served(args, threads)
         return
     specs, iterations, substeps, frame_dt = workload_specs(args.workload, args.seed)
+    if args.scenes > 0:
+        specs = specs[:args.scenes]
 
     if args.impl == "reference":
         if rank != 0:

@@ -394,9 +394,11 @@ oct_status oct_torsion_profile(int32_t element, const float* rest, const float* 
                                float* distance, float* angles, int32_t capacity, int32_t* count);
 
 /* Checkpoint / restore of one scene (new; the reference's DataRecorder writes no restorable
- * state): per node the displacement, the start-of-sub-step displacement, the velocity and the
- * fixed mask, then the fixation groups, the effects' stretch distances, the multigrid schedule
- * and the pending initial velocity.  A restored scene continues exactly as the saved one. */
+ * state): a 4-float header (format tag, node count, element count, element type), then per
+ * node the displacement, the start-of-sub-step displacement, the velocity and the fixed mask,
+ * then the fixation groups, the effects' stretch distances, the multigrid schedule and the
+ * pending initial velocity.  A restored scene continues exactly as the saved one; restore
+ * checks the header first and refuses (OCT_EINVAL) a checkpoint of a scene of another shape. */
 oct_status oct_scene_state_size(oct_scene* s, size_t* n_floats);
 oct_status oct_scene_save(oct_scene* s, float* out);
 oct_status oct_scene_restore(oct_scene* s, const float* in);
@@ -419,8 +421,8 @@ oct_status oct_batch_group_info(oct_batch* b, int g, int32_t* element, int32_t* 
  * state advances as in an iteration) and returns their total device time (CUDA events). */
 oct_status oct_batch_time_group(oct_batch* b, int g, int sweeps, float dt, float* ms);
 
-/* Allocation-free FP64 elastic energy (no counterpart in the reference; the reference has
- * no energy evaluator).  For callers that must not allocate device memory when they call
+/* Allocation-free FP64 elastic energy (no counterpart entry point in the reference; its CPU
+ * materials' get_energy, FEM_ContinuousMaterial.cpp:10-87, give the densities).  For callers that must not allocate device memory when they call
  * it: a host application whose device memory belongs to its own pool and which forbids
  * driver allocations inside its frame loop, or a real-time loop that cannot take the
  * latency and implicit synchronisation of cudaMalloc/cudaFree.  Computes

@@ -69,6 +69,7 @@ struct SceneDev {
     int n_nodes, n_elements, n_fixed, element;
     int eq_stride;                     // records per element: NQ, or 1 for affine elements
     const float4* ent;                 // owner entries in slot order (EntryLayout), or null
+    const float4* rtab;                // distinct quadrature records of affine elements (3 float4 each)
     float damping;      // k_d
     float gx, gy, gz;
     float bminx, bminy, bminz, bmaxx, bmaxy, bmaxz;
@@ -96,22 +97,44 @@ struct VWork {
     int pad0, pad1;
 };
 
-// Owner entries (packed mapping): one record per (vertex, owner) pair in slot order,
-// contiguous per warp item so a single bulk copy stages a whole item in shared memory:
-// the owner element's NE node ids, the vertex's local index r, the element id, and (affine
-// scenes) the element's 12-float quadrature record; padded to a multiple of 4 words.
+// Owner entries: one per (vertex, owner) pair in slot order, contiguous per vertex (and per
+// warp item of the packed mapping, so one bulk copy stages a whole item in shared memory).
+// An entry holds the owner element's node ids and an index into the scene's record table
+// instead of the record itself: the quadrature record (JX_inv, V, lambda, mu; for P1 the
+// G_j vectors, V, lambda, mu of the vertex's corner) of every affine element is stored once
+// per distinct value (SceneDev::rtab), so a mesh whose elements repeat a few shapes (the
+// generated beams and cubes: 6 tetrahedron shapes, 1 hexahedron) streams only node ids.  For
+// non-affine elements the index is the element id into the per-point records (SceneDev::eq).
+// Node ids take the low kIdBits bits of a word; the spare high bits carry the local index and
+// the record index in the entries that have no room for separate words (P1, Q1).
+constexpr int kIdBits = 27;
+constexpr int kIdMask = (1 << kIdBits) - 1;
+constexpr int kSpareBits = 32 - kIdBits;
 template <int NE> struct EntryLayout {
-    static constexpr int kIds = 0, kR = NE, kEid = NE + 1, kRec = NE + 2;
-    static constexpr int kWords = ((NE + 2 + 12) + 3) / 4 * 4;
+    // node ids, then r, then the record index; padded to a multiple of 4 words
+    static constexpr int kIds = 0, kR = NE, kRec = NE + 1;
+    static constexpr int kWords = ((NE + 2) + 3) / 4 * 4;
+    static constexpr long long kMaxRecords = 1ll << 31;
 };
-// P1 (one quadrature point, always affine) entries are 64 B: the node ids with the vertex's
-// own node first, then G_j = JX_inv^T dN_j of the three other nodes in that order (9 floats),
-// V, lambda, mu.  Since sum_i dN_i = 0, F = I + sum_j (u_j - u_own) (x) G_j and the vertex's
-// own g = -(G_1 + G_2 + G_3): no local index, element id or JX_inv needed.
+// P1: the four node ids with the vertex's own node first; the record index (of the
+// element's record for that corner: G_j = JX_inv^T dN_j of the three other nodes in order,
+// V, lambda, mu; since sum_i dN_i = 0, F = I + sum_j (u_j - u_own) (x) G_j and the vertex's
+// own g = -(G_1 + G_2 + G_3)) is split over the ids' spare bits: 16 B per entry.
 template <> struct EntryLayout<4> {
-    static constexpr int kIds = 0, kG = 4, kV = 13, kLam = 14, kMu = 15;
-    static constexpr int kWords = 16;
+    static constexpr int kIds = 0;
+    static constexpr int kWords = 4;
+    static constexpr long long kMaxRecords = 1ll << (4 * kSpareBits);
 };
+// Q1: eight node ids; r in the spare bits of the first, the record index in those of the
+// other seven: 32 B per entry.
+template <> struct EntryLayout<8> {
+    static constexpr int kIds = 0;
+    static constexpr int kWords = 8;
+    static constexpr long long kMaxRecords = 1ll << 31;
+};
+inline constexpr int entry_words(int ne) {
+    return ne == 4 ? EntryLayout<4>::kWords : ne == 8 ? EntryLayout<8>::kWords : ((ne + 2) + 3) / 4 * 4;
+}
 
 // One unit of node-parallel work (predictor, velocity update, Chebyshev).
 struct NWork {

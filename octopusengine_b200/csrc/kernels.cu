@@ -355,22 +355,44 @@ __device__ __forceinline__ void owner_terms(const SceneDev& S, int packed, const
     element_terms<E, MAT>(ux, uy, uz, r, A, B, C, rec, S.eq_stride == 1, s_dN, mixed, acc, cmp, stream);
 }
 
-// Owner given as a staged entry (EntryLayout) in shared memory.
+// Owner entry fields (EntryLayout): node ids in the low kIdBits bits; r and the record index
+// in separate words, or (P1, Q1) in the ids' spare bits.
+__device__ __forceinline__ int entry_node(const float* en, int i) { return __float_as_int(en[i]) & kIdMask; }
+__device__ __forceinline__ unsigned entry_spare(const float* en, int i) { return (unsigned)__float_as_int(en[i]) >> kIdBits; }
+template <int NE> __device__ __forceinline__ int entry_r(const float* en) {
+    if constexpr (NE == 4) return 0;   // own node first
+    else if constexpr (NE == 8) return (int)entry_spare(en, 0);
+    else return __float_as_int(en[EntryLayout<NE>::kR]);
+}
+template <int NE> __device__ __forceinline__ int entry_rec(const float* en) {
+    if constexpr (NE == 4) {
+        return (int)(entry_spare(en, 0) | entry_spare(en, 1) << kSpareBits | entry_spare(en, 2) << (2 * kSpareBits) |
+                     entry_spare(en, 3) << (3 * kSpareBits));
+    } else if constexpr (NE == 8) {
+        unsigned v = 0;
+#pragma unroll
+        for (int j = 1; j < 8; ++j) v |= entry_spare(en, j) << (kSpareBits * (j - 1));
+        return (int)(v & 0x7fffffffu);
+    } else {
+        return __float_as_int(en[EntryLayout<NE>::kRec]);
+    }
+}
+
+// Owner given as an entry (EntryLayout), staged in shared memory or held in registers.
 template <int E, int MAT>
 __device__ __forceinline__ void entry_terms(const SceneDev& S, const float* __restrict__ en, const float* __restrict__ s_dN,
                                             bool mixed, float acc[9], float cmp[9]) {
-    constexpr int NE = ElemT<E>::NE;
-    using L = EntryLayout<NE>;
+    constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ;
     const unsigned long long keep = policy_keep(), stream = policy_stream();
-    if constexpr (NE == 4) {   // compact P1 entry: own node first, G_j of the other three
-        const float4 u0 = ld_hint(&S.u[__float_as_int(en[L::kIds])], keep);
-        const float4 u1 = ld_hint(&S.u[__float_as_int(en[L::kIds + 1])], keep);
-        const float4 u2 = ld_hint(&S.u[__float_as_int(en[L::kIds + 2])], keep);
-        const float4 u3 = ld_hint(&S.u[__float_as_int(en[L::kIds + 3])], keep);
+    if constexpr (NE == 4) {   // P1: own node first, the corner's record holds G_j of the other three
+        const float4 u0 = ld_hint(&S.u[entry_node(en, 0)], keep);
+        const float4 u1 = ld_hint(&S.u[entry_node(en, 1)], keep);
+        const float4 u2 = ld_hint(&S.u[entry_node(en, 2)], keep);
+        const float4 u3 = ld_hint(&S.u[entry_node(en, 3)], keep);
+        const float4* R = S.rtab + 3 * (size_t)entry_rec<NE>(en);
+        const float4 R0 = ld_hint(R, keep), R1 = ld_hint(R + 1, keep), R2 = ld_hint(R + 2, keep);
         const V3 d1 = xyz(u1) - xyz(u0), d2 = xyz(u2) - xyz(u0), d3 = xyz(u3) - xyz(u0);
-        const V3 g1 = mk(en[L::kG], en[L::kG + 1], en[L::kG + 2]);
-        const V3 g2 = mk(en[L::kG + 3], en[L::kG + 4], en[L::kG + 5]);
-        const V3 g3 = mk(en[L::kG + 6], en[L::kG + 7], en[L::kG + 8]);
+        const V3 g1 = mk(R0.x, R0.y, R0.z), g2 = mk(R0.w, R1.x, R1.y), g3 = mk(R1.z, R1.w, R2.x);
         // F_b = e_b + sum_j d_j G_j[b]
         V3 F0 = d1 * g1.x + d2 * g2.x + d3 * g3.x;
         V3 F1 = d1 * g1.y + d2 * g2.y + d3 * g3.y;
@@ -378,7 +400,7 @@ __device__ __forceinline__ void entry_terms(const SceneDev& S, const float* __re
         F0.x += 1.f; F1.y += 1.f; F2.z += 1.f;
         const V3 g = mk(-(g1.x + g2.x + g3.x), -(g1.y + g2.y + g3.y), -(g1.z + g2.z + g3.z));
         float t[9];
-        material_terms<MAT>(F0, F1, F2, g, en[L::kLam], en[L::kMu], en[L::kV] * wq<E>(0), t);
+        material_terms<MAT>(F0, F1, F2, g, R2.z, R2.w, R2.y * wq<E>(0), t);
         if (mixed) {
 #pragma unroll
             for (int k = 0; k < 3; ++k) kadd(acc[k], cmp[k], t[k]);
@@ -393,22 +415,17 @@ __device__ __forceinline__ void entry_terms(const SceneDev& S, const float* __re
     float ux[NE], uy[NE], uz[NE];
 #pragma unroll
     for (int i = 0; i < NE; ++i) {
-        const float4 t = ld_hint(&S.u[__float_as_int(en[L::kIds + i])], keep);
+        const float4 t = ld_hint(&S.u[entry_node(en, i)], keep);
         ux[i] = t.x; uy[i] = t.y; uz[i] = t.z;
     }
-    const int r = __float_as_int(en[L::kR]);
+    const int r = entry_r<NE>(en), rec = entry_rec<NE>(en);
     const bool affine = S.eq_stride == 1;
-    float4 A, B, C;
-    const float4* rec = nullptr;
-    if (affine) {
-        A = make_float4(en[L::kRec], en[L::kRec + 1], en[L::kRec + 2], en[L::kRec + 3]);
-        B = make_float4(en[L::kRec + 4], en[L::kRec + 5], en[L::kRec + 6], en[L::kRec + 7]);
-        C = make_float4(en[L::kRec + 8], en[L::kRec + 9], en[L::kRec + 10], en[L::kRec + 11]);
-    } else {
-        rec = S.eq + (size_t)__float_as_int(en[L::kEid]) * S.eq_stride * 3;
-        A = ld_hint(rec, stream); B = ld_hint(rec + 1, stream); C = ld_hint(rec + 2, stream);
-    }
-    element_terms<E, MAT>(ux, uy, uz, r, A, B, C, rec, affine, s_dN, mixed, acc, cmp, stream);
+    // affine: the element's record in the table of distinct records (small, cached);
+    // otherwise rec is the element id into its per-point records
+    const float4* R = affine ? S.rtab + 3 * (size_t)rec : S.eq + (size_t)rec * NQ * 3;
+    const float4 A = ld_hint(R, affine ? keep : stream), B = ld_hint(R + 1, affine ? keep : stream),
+                 C = ld_hint(R + 2, affine ? keep : stream);
+    element_terms<E, MAT>(ux, uy, uz, r, A, B, C, R, affine, s_dN, mixed, acc, cmp, stream);
     }
 }
 
@@ -575,8 +592,7 @@ __global__ void __launch_bounds__(kBlock, MinBlocks<E>::value) k_vertex_packed(c
         int vid = 0;
         bool active = false;
         if (lane < wk.n_pairs) {
-            if constexpr (NE == 4) vid = __float_as_int(en[EntryLayout<NE>::kIds]);   // own node first
-            else vid = __float_as_int(en[EntryLayout<NE>::kIds + __float_as_int(en[EntryLayout<NE>::kR])]);
+            vid = entry_node(en, entry_r<NE>(en));
             active = mode == 2 || S.mask[vid] != 0;
         }
         float acc[9], cmp[9];
@@ -621,7 +637,18 @@ template <int E> constexpr int packed_smem_bytes() { return (kBlock / 32) * 2 * 
 // mode 0: VBD solve; mode 1: VBD residual (r into u_new, |r| reductions); mode 2: explicit force.
 // Resident blocks per SM the lane-group kernel is compiled for: P2 and Q1 are held to 128
 // registers (4 blocks, 16 warps per SM; ptxas spills a few bytes), P1 to 80.
-template <int E> struct LaneMinBlocks { static constexpr int value = E == 3 ? 6 : (E == 6 || E == 7 ? 4 : 1); };
+#ifndef OCTB_P2_MIN_BLOCKS
+#define OCTB_P2_MIN_BLOCKS 4
+#endif
+#ifndef OCTB_Q1_MIN_BLOCKS
+#define OCTB_Q1_MIN_BLOCKS 4
+#endif
+#ifndef OCTB_P1_MIN_BLOCKS
+#define OCTB_P1_MIN_BLOCKS 6
+#endif
+template <int E> struct LaneMinBlocks {
+    static constexpr int value = E == 3 ? OCTB_P1_MIN_BLOCKS : (E == 6 ? OCTB_Q1_MIN_BLOCKS : (E == 7 ? OCTB_P2_MIN_BLOCKS : 1));
+};
 
 template <int E, int MAT>
 __global__ void __launch_bounds__(kBlock, LaneMinBlocks<E>::value) k_vertex(const SceneDev* __restrict__ scenes, const VWork* __restrict__ work,

@@ -173,6 +173,9 @@ extern "C" oct_status oct_elastic_energy_noalloc(int element, int material, cons
     const double lam = Y * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = Y / (2.0 * (1.0 + nu));
     cudaStream_t st = (cudaStream_t)stream;
     const int threads = 128, blocks = (n_elements + threads - 1) / threads < 4096 ? (n_elements + threads - 1) / threads : 4096;
+    // a launch error left on this thread by an earlier call is not this call's failure: clear
+    // it so the checks after the launches see only their own
+    (void)cudaGetLastError();
     switch (element) {
         case 3: k_element_energy<3><<<blocks, threads, 0, st>>>(d_positions, d_rest_positions, d_topology, n_elements, material, lam, mu, scratch); break;
         case 6: k_element_energy<6><<<blocks, threads, 0, st>>>(d_positions, d_rest_positions, d_topology, n_elements, material, lam, mu, scratch); break;
@@ -181,6 +184,7 @@ extern "C" oct_status oct_elastic_energy_noalloc(int element, int material, cons
         case 9: k_element_energy<9><<<blocks, threads, 0, st>>>(d_positions, d_rest_positions, d_topology, n_elements, material, lam, mu, scratch); break;
         default: return OCT_EINVAL;
     }
+    if (cudaGetLastError() != cudaSuccess) return OCT_ECUDA;
     k_fixed_order_sum<<<1, 1024, 0, st>>>(scratch, n_elements, d_out);
     return cudaGetLastError() == cudaSuccess ? OCT_OK : OCT_ECUDA;
 }

@@ -3,6 +3,7 @@
 // reference's launch structure, and batches that step many scenes through one launch per
 // (element type, colour) captured in a CUDA graph.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -13,6 +14,7 @@
 #include <random>
 #include <sstream>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <nvtx3/nvToolsExt.h>
@@ -138,6 +140,7 @@ struct oct_scene {
     oct_ctx* ctx = nullptr;
     DevMem mem;
     int solver = 0, element = 0, material = 0, ne = 0, nq = 0;
+    int64_t n_records = 0;          // distinct quadrature records the owner entries index
     int n_nodes = 0, n_elements = 0, n_fixed = 0, n_colors = 0;
     int iterations = 1, order_mode = 0, tpv = 8, precision = 0, max_valence = 0;
     float rho = 0.f, global_damping = 0.f;
@@ -315,6 +318,7 @@ oct_status build_vertex_work(oct_scene* s) {
 }
 
 oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s);
+
 
 // Multigrid VBD (MG_VBD_FEM ctor, octopus/src/Dynamic/VBD/MG_VertexBlockDescent.cpp:134-176):
 // the linear level is built as a scene of the corner nodes (numbered in ascending order)
@@ -580,7 +584,8 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     s->vids = slot_vids;   // the reference order (GPU_VBD_FEM::create_buffers), reported by the getters
     // processing order: within each colour, vertices by decreasing owner count (ascending id
     // among equals), so the lanes of a warp get similar loads; results do not depend on the
-    // order inside a colour
+    // order inside a colour.  (A Morton order of the rest positions among equals, tried so
+    // that a warp's vertices share element nodes in L1, was not faster.)
     if (d->solver != OCT_SOLVER_XPBD) {
         std::vector<int32_t> val(N, 0);
         for (int64_t k = 0; k < (int64_t)E * NE; ++k) val[d->topology[k]]++;
@@ -654,44 +659,94 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     h.bmaxx = d->box_max[0]; h.bmaxy = d->box_max[1]; h.bmaxz = d->box_max[2];
     h.box_limit = s->box;
     h.precision = s->precision;
-    // owner entries in slot order for the packed mapping (EntryLayout in device.cuh)
+    // owner entries in slot order (EntryLayout in device.cuh) and the table of distinct
+    // records they index; without entries (node ids past kIdBits, or more distinct P1 corner
+    // records than the P1 entry can index) the colour kernels read owners, topology and records
     h.ent = nullptr;
-    {
-        const bool p1 = NE == 4;   // compact 64 B P1 entries (EntryLayout<4>)
-        const int EW = p1 ? 16 : ((NE + 2 + 12) + 3) / 4 * 4;
+    h.rtab = nullptr;
+    if ((int64_t)N <= (int64_t)kIdMask + 1) {
+        const int EW = entry_words(NE);
+        const bool affine = h.eq_stride == 1;
+        // distinct records, compared bit for bit (identical records give identical results)
+        struct KeyHash {
+            size_t operator()(const std::array<uint32_t, 12>& k) const {
+                uint64_t h = 1469598103934665603ull;
+                for (uint32_t v : k) { h ^= v; h *= 1099511628211ull; }
+                return (size_t)h;
+            }
+        };
+        std::unordered_map<std::array<uint32_t, 12>, int32_t, KeyHash> index;
+        std::vector<float4> rtab;
+        auto intern = [&](const float* rec12) {
+            std::array<uint32_t, 12> k;
+            std::memcpy(k.data(), rec12, sizeof(k));
+            auto it = index.find(k);
+            if (it != index.end()) return it->second;
+            const int32_t id = (int32_t)(rtab.size() / 3);
+            index.emplace(k, id);
+            rtab.push_back(make_float4(rec12[0], rec12[1], rec12[2], rec12[3]));
+            rtab.push_back(make_float4(rec12[4], rec12[5], rec12[6], rec12[7]));
+            rtab.push_back(make_float4(rec12[8], rec12[9], rec12[10], rec12[11]));
+            return id;
+        };
+        std::vector<int32_t> erec;   // per element (affine, not P1): its record index
+        if (affine && NE != 4) {
+            erec.resize(E);
+            for (int e = 0; e < E; ++e) erec[e] = intern(reinterpret_cast<const float*>(&eq[(size_t)e * 3]));
+        }
         std::vector<float4> ent((size_t)owners.size() * EW / 4, make_float4(0, 0, 0, 0));
-        for (size_t o = 0; o < owners.size(); ++o) {
-            float* e = reinterpret_cast<float*>(&ent[o * EW / 4]);
-            int32_t* ei = reinterpret_cast<int32_t*>(e);
+        bool ok = true;
+        for (size_t o = 0; o < owners.size() && ok; ++o) {
+            int32_t* ei = reinterpret_cast<int32_t*>(&ent[o * EW / 4]);
             const int eid = owners[o] >> kOwnerShift, r = owners[o] & ((1 << kOwnerShift) - 1);
-            if (p1) {
+            const int32_t* te = &topo[(size_t)eid * NE];
+            if (NE == 4) {
                 // own node first, then the others in element order with G_j = JX_inv^T dN_j
                 // (FP64 from the stored JX_inv columns m_b; dN_j from the shape table)
                 const float* m = reinterpret_cast<const float*>(&eq[(size_t)eid * 3]);
-                ei[0] = topo[(size_t)eid * NE + r];
+                float rec[12];
+                ei[0] = te[r];
                 for (int i = 0, j = 1; i < NE; ++i) {
                     if (i == r) continue;
-                    ei[j] = topo[(size_t)eid * NE + i];
+                    ei[j] = te[i];
                     const double* dn = &sh.dN[(size_t)i * 3];
                     for (int b = 0; b < 3; ++b)
-                        e[4 + 3 * (j - 1) + b] = (float)((double)m[3 * b] * dn[0] + (double)m[3 * b + 1] * dn[1] +
-                                                         (double)m[3 * b + 2] * dn[2]);
+                        rec[3 * (j - 1) + b] = (float)((double)m[3 * b] * dn[0] + (double)m[3 * b + 1] * dn[1] +
+                                                       (double)m[3 * b + 2] * dn[2]);
                     ++j;
                 }
-                e[13] = m[9];    // V
-                e[14] = m[10];   // lambda
-                e[15] = m[11];   // mu
+                rec[9] = m[9];     // V
+                rec[10] = m[10];   // lambda
+                rec[11] = m[11];   // mu
+                const int32_t id = intern(rec);
+                if ((long long)id >= (1ll << (4 * kSpareBits))) { ok = false; break; }
+                for (int j = 0; j < 4; ++j) ei[j] |= (int32_t)(((uint32_t)id >> (kSpareBits * j)) & ((1u << kSpareBits) - 1)) << kIdBits;
                 continue;
             }
-            for (int i = 0; i < NE; ++i) ei[i] = topo[(size_t)eid * NE + i];
-            ei[NE] = r;
-            ei[NE + 1] = eid;
-            if (h.eq_stride == 1) std::memcpy(e + NE + 2, &eq[(size_t)eid * 3], 12 * sizeof(float));
+            const int32_t rec = affine ? erec[eid] : eid;
+            for (int i = 0; i < NE; ++i) ei[i] = te[i];
+            if (NE == 8) {
+                ei[0] |= r << kIdBits;
+                for (int j = 1; j < 8; ++j)
+                    ei[j] |= (int32_t)((((uint64_t)(uint32_t)rec) >> (kSpareBits * (j - 1))) & ((1u << kSpareBits) - 1)) << kIdBits;
+            } else {
+                ei[NE] = r;
+                ei[NE + 1] = rec;
+            }
         }
-        float4* entd;
-        if ((st = upload(c, s->mem, entd, ent))) return st;
-        h.ent = entd;
+        if (ok) {
+            float4* entd;
+            if ((st = upload(c, s->mem, entd, ent))) return st;
+            h.ent = entd;
+            if (!rtab.empty()) {
+                float4* rtd;
+                if ((st = upload(c, s->mem, rtd, rtab))) return st;
+                h.rtab = rtd;
+            }
+            s->n_records = (int64_t)rtab.size() / 3;
+        }
     }
+    if (!h.ent && s->tpv == 0) s->tpv = default_tpv(d->element);   // the packed mapping streams entries
     for (int k = 0; k < kMaxEffects; ++k) { s->effects[k] = EffectDev{}; s->effects[k].kind = -1; }
     if ((st = upload(c, s->mem, s->d_effects, std::vector<EffectDev>(s->effects, s->effects + kMaxEffects)))) return st;
     h.effects = s->d_effects;
@@ -965,7 +1020,8 @@ oct_status oct_scene_footprint(const oct_scene_desc* d, size_t* bytes) {
     const size_t N = d->n_nodes, E = d->n_elements;
     size_t b = N * (6 * sizeof(float4) + 3 * sizeof(int)) + (d->rho > 0.f ? 2 * N * sizeof(float4) : 0);
     b += E * ne * sizeof(int) * 2 + E * nq * 3 * sizeof(float4);   // topology, owners, quadrature records
-    b += E * ne * (size_t)(((ne + 2 + 12) + 3) / 4 * 4) * sizeof(float);   // owner entries
+    b += E * ne * (size_t)entry_words(ne) * sizeof(float);                  // owner entries
+    b += (ne == 4 ? 4 : 1) * E * 3 * sizeof(float4);                        // distinct records, at most
     b += (N / 16 + 64) * sizeof(VWork) + (N / 256 + 8) * 2 * sizeof(NWork) + (size_t)std::max(d->n_fixed, 0) * sizeof(int);
     b += 4096;   // descriptors and reduction scratch
     *bytes = b;
@@ -1244,9 +1300,14 @@ oct_status oct_ctx_wait_probe(oct_ctx* c, int32_t limit) {
 // Checkpoint: per node u, u_last, v (9 floats) and the mask, then the fixation table
 // (kFixGroups x 16), the effects' stretch distances (kMaxEffects), the multigrid schedule (3)
 // and the pending initial-velocity flag.
+// Checkpoint header: a format tag and the scene's shape, checked by restore before it reads
+// anything else, so a checkpoint of another scene is refused instead of read past its end.
+constexpr int32_t kCheckpointTag = 0x3154434F;   // "OCT1", stored as the bits of a float
+constexpr int kCheckpointHeader = 4;              // tag, n_nodes, n_elements, element
+
 oct_status oct_scene_state_size(oct_scene* s, size_t* n_floats) {
     if (!s || !n_floats) return OCT_EINVAL;
-    *n_floats = (size_t)s->n_nodes * 10 + kFixGroups * 16 + kMaxEffects + 4;
+    *n_floats = kCheckpointHeader + (size_t)s->n_nodes * 10 + kFixGroups * 16 + kMaxEffects + 4;
     return OCT_OK;
 }
 
@@ -1262,6 +1323,8 @@ oct_status oct_scene_save(oct_scene* s, float* out) {
     OCT_CUDA(c, cudaMemcpy(v.data(), s->h.v, sizeof(float4) * N, cudaMemcpyDeviceToHost));
     OCT_CUDA(c, cudaMemcpy(mask.data(), s->h.mask, sizeof(int) * N, cudaMemcpyDeviceToHost));
     float* o = out;
+    std::memcpy(o++, &kCheckpointTag, sizeof(float));
+    *o++ = (float)N; *o++ = (float)s->n_elements; *o++ = (float)s->element;
     for (int i = 0; i < N; ++i) {
         *o++ = u[i].x; *o++ = u[i].y; *o++ = u[i].z;
         *o++ = ul[i].x; *o++ = ul[i].y; *o++ = ul[i].z;
@@ -1284,9 +1347,13 @@ oct_status oct_scene_restore(oct_scene* s, const float* in) {
     if (!s || !in) return OCT_EINVAL;
     oct_ctx* c = s->ctx;
     const int N = s->n_nodes;
+    int32_t tag = 0;
+    std::memcpy(&tag, in, sizeof(float));
+    if (tag != kCheckpointTag || in[1] != (float)N || in[2] != (float)s->n_elements || in[3] != (float)s->element)
+        return fail(c, OCT_EINVAL, "checkpoint of another scene (or not a checkpoint)");
     std::vector<float4> u(N), ul(N), v(N);
     std::vector<int> mask(N);
-    const float* p = in;
+    const float* p = in + kCheckpointHeader;
     for (int i = 0; i < N; ++i, p += 10) {
         u[i] = make_float4(p[0], p[1], p[2], 0.f);
         ul[i] = make_float4(p[3], p[4], p[5], 0.f);
@@ -1673,6 +1740,10 @@ oct_status oct_scene_set_mapping(oct_scene* s, int tpv) {
         if (tpv < 0) return fail(s->ctx, OCT_ENOTSUP, "packed mapping needs at most 32 owners per vertex");
         t = s->max_valence > 64 ? 32 : default_tpv(s->element);
     }
+    if (t == 0 && !s->h.ent) {
+        if (tpv < 0) return fail(s->ctx, OCT_ENOTSUP, "packed mapping needs owner entries (scene past their index range)");
+        t = default_tpv(s->element);
+    }
     OCT_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
     s->tpv = t;
     drop_frame_graph(s);
@@ -1717,9 +1788,10 @@ oct_status oct_autotune_mapping(oct_ctx* c, oct_scene* const* scenes, int n, flo
     }
     for (auto& [element, list] : by_element) {
         int max_val = 0;
-        for (auto* s : list) max_val = std::max(max_val, s->max_valence);
+        bool entries = true;
+        for (auto* s : list) { max_val = std::max(max_val, s->max_valence); entries = entries && s->h.ent; }
         std::vector<int> cands = {1, 2, 4, 8, 16, 32};
-        if (max_val <= 32) cands.insert(cands.begin(), -1);
+        if (max_val <= 32 && entries) cands.insert(cands.begin(), -1);
         const std::vector<int> old = [&] { std::vector<int> v; for (auto* s : list) v.push_back(s->tpv); return v; }();
         float best_ms = 1e30f;
         int best = 0;

@@ -78,3 +78,21 @@ def test_checkpoint_restore_reproduces_the_run(ctx, kind):
         s.step(1 / 60, 3)
     np.testing.assert_array_equal(s.get_position(), a[0])
     np.testing.assert_array_equal(s.get_velocity(), a[1])
+
+
+def test_restore_refuses_a_checkpoint_of_another_scene(ctx):
+    from octopusengine_b200 import capi
+    import octopusengine_b200 as ob
+    a, _, _, _ = pair(ctx, O.HEXA, cells=(3, 2, 2), iterations=3)
+    b, _, _, _ = pair(ctx, O.HEXA, cells=(4, 2, 2), iterations=3)
+    a.step(1 / 60, 1)
+    snap = a.save()
+    assert snap.size == a.save().size
+    with pytest.raises(ob.OctError) as e:
+        b.restore(snap)
+    assert e.value.status == capi.EINVAL
+    with pytest.raises(ob.OctError):
+        b.restore(np.zeros(b.save().size, np.float32))   # not a checkpoint at all
+    before = b.get_position()
+    b.step(1 / 60, 1)   # the refused restores left b untouched
+    assert np.isfinite(b.get_position()).all() and not np.array_equal(before, b.get_position())
