@@ -500,6 +500,44 @@ def single_scene_p2(ctx, seed, stream, warmup=3, steps=5):
     return out
 
 
+def batched_xpbd(ctx, specs, seed, stream, threads, warmup=3, steps=5, substeps=5, frame_dt=FRAME_DT):
+    """The batched workload's scenes as XPBD scenes (reference default OptiShared: V0 for P1, the
+    raw V2 update for P2/Q1) in one batch: per 1/60 s frame 5 sub-steps of GPU_PBD::step over
+    all scenes, one launch per (element type, material, update form, colour) across the scenes,
+    the sub-step a CUDA graph.  Metric: element projections/s (both constraints of one
+    element, every element once per sub-step)."""
+    import torch
+    import octopusengine_b200 as ob
+    t0 = time.time()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        scenes = list(ex.map(lambda a: build_scene(ctx, a[1], 1, ob.PREC_PLAIN, seed + a[0], solver=ob.SOLVER_XPBD),
+                             enumerate(specs)))
+    setup_s = time.time() - t0
+    b = ob.Batch(ctx, scenes)
+    units = sum(s.n_elements for s in scenes) * substeps
+    for _ in range(warmup):
+        b.step(frame_dt, substeps)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    l0 = ctx.launch_count()
+    ev[0].record(stream)
+    for k in range(steps):
+        b.step(frame_dt, substeps)
+        ev[k + 1].record(stream)
+    torch.cuda.synchronize()
+    launches = ctx.launch_count() - l0
+    ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+    total = ev[0].elapsed_time(ev[-1])
+    status = b.status()
+    b.close()
+    for s in scenes:
+        s.close()
+    return {"value": units * steps / (total * 1e-3), "unit": "element-projections/s", "scenes": len(specs),
+            "elements": units // substeps, "substeps": substeps, "frame_dt": frame_dt, "ms_per_frame": total / steps,
+            "p50_frame_ms": float(np.percentile(ms, 50)), "p99_frame_ms": float(np.percentile(ms, 99)),
+            "gpu_launches": int(launches), "failed_scenes": int((status != 0).sum()), "setup_s": setup_s}
+
+
 def bench_served(args, threads):
     """Continuous batching of a Poisson request stream through oct_server_* (one GPU)."""
     import ctypes as C
@@ -870,9 +908,10 @@ def main():
                  "path": "each scene stepped alone through oct_scene_step: FP32, one launch per colour, no graph"}
 
     # ---- the rest of the metric on the same GPU: config 2 alone, and a short served stream
-    p2_line, served_line = None, None
+    p2_line, served_line, xpbd_line = None, None, None
     if rank == 0 and world == 1 and args.workload == "batched" and not args.no_extra:
         p2_line = single_scene_p2(ctx, args.seed, stream)
+        xpbd_line = batched_xpbd(ctx, specs, args.seed, stream, threads)
         served_line = served_stream(ctx, args.serve_rate, args.serve_window, args.seed, threads)
 
     cpu, parity = None, None
@@ -917,6 +956,7 @@ def main():
             "cpu_baseline": cpu,
             "parity": parity,
             "p2_single": p2_line,
+            "xpbd_batched": xpbd_line,
             "served": served_line,
             "setup_s": setup_s,
         }

@@ -233,9 +233,12 @@ oct_status oct_scene_vertex_residuals(oct_scene* s, float dt, float* out_n3);
  * unsolved), else the context's own error word (OCT_OK when clear). */
 oct_status oct_scene_status(oct_scene* s);
 
-/* Batch: many VBD scenes stepped together, one launch per (element type, colour) across all
- * scenes, driven by a per-scene work table, the sub-step captured as a CUDA graph.  All
- * scenes must be VBD scenes of this context with equal iteration counts. */
+/* Batch: many scenes stepped together, one launch per (element type, colour) across all
+ * scenes, driven by a per-scene work table, the sub-step captured as a CUDA graph.  The
+ * scenes are all VBD scenes of this context with equal iteration counts, or all XPBD scenes
+ * (GPU_PBD::step over every scene: one launch per (element type, material, update form,
+ * colour) with the element colours of all scenes, each scene with its own global damping);
+ * explicit scenes are stepped alone (OCT_ENOTSUP). */
 /* Lane mapping of a VBD or explicit scene's vertex kernel (same values as
  * oct_scene_desc.threads_per_vertex: -1 packed pairs, 0 measured default, 1..32 lanes per
  * vertex).  OCT_ENOTSUP for the packed mapping when a vertex has more than 32 owners. */

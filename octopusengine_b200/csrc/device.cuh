@@ -77,6 +77,17 @@ struct SceneDev {
     int precision;                     // 0 plain, 1 mixed
     EffectDev* effects;                // kMaxEffects slots (scene memory)
     int* status;                       // per-scene failure flags: kStatusTimeout, kStatusNonFinite
+    const int* elems;                  // XPBD: element ids sorted by colour
+    float global_damping;              // XPBD velocity damping (GPU_PBD global_damping)
+};
+
+// One block of XPBD element work: `count` consecutive entries of one scene's colour-sorted
+// element list from `begin` (at most the kernel's elements per block).
+struct XWork {
+    int scene;
+    int begin;
+    int count;
+    int pad;
 };
 
 // Per-scene failure flags (SceneDev::status), read and cleared by the host after a frame.

@@ -764,8 +764,8 @@ __global__ void k_predict(const SceneDev* __restrict__ scenes, const NWork* __re
 }
 
 // kernel_velocity_update (GPU_VBD.cu:20-25); with global damping for XPBD (GPU_PBD.cu:8-18).
-__global__ void k_velocity(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work, int n_work,
-                           float global_damping, int pbd, StepParams P) {
+__global__ void k_velocity(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work, int n_work, int pbd,
+                           StepParams P) {
     pdl_trigger();
     pdl_wait();
     const NWork wk = work[blockIdx.x];
@@ -777,7 +777,7 @@ __global__ void k_velocity(const SceneDev* __restrict__ scenes, const NWork* __r
     if (pbd) {
         const float nv = sqrtf(v.x * v.x + v.y * v.y + v.z * v.z);
         if (nv > 1e-7f) {
-            const float coef = global_damping * P.dt / S.y[i].w;
+            const float coef = S.global_damping * P.dt / S.y[i].w;
             const float d = -nv * (coef > 1.f ? 1.f : coef);
             v.x += v.x / nv * d; v.y += v.y / nv * d; v.z += v.z / nv * d;
         }
@@ -1142,8 +1142,8 @@ template <int G> __device__ __forceinline__ float group_sum(float v) {
 }
 
 template <int E, int MAT, bool RAW>
-__global__ void __launch_bounds__(kBlock) k_xpbd(const SceneDev* __restrict__ scenes, const int* __restrict__ elems,
-                                                 int begin, int count, int scene, StepParams P) {
+__global__ void __launch_bounds__(kBlock) k_xpbd(const SceneDev* __restrict__ scenes, const XWork* __restrict__ work,
+                                                 StepParams P) {
     constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ, G = XpbdLanes<E>::G, GPB = kBlock / G;
     constexpr int NI = (NE + G - 1) / G;   // nodes per lane
     static_assert(NQ <= G, "one quadrature point per lane");
@@ -1156,10 +1156,10 @@ __global__ void __launch_bounds__(kBlock) k_xpbd(const SceneDev* __restrict__ sc
     pdl_wait();
 
     const int lane = threadIdx.x % G, grp = threadIdx.x / G;
-    const int t = blockIdx.x * GPB + grp;
-    const bool active = t < count;   // no early exit: every lane takes part in the shuffles
-    const SceneDev& S = scenes[scene];
-    const int eid = active ? elems[begin + t] : 0;
+    const XWork wk = work[blockIdx.x];   // GPB elements of one scene's colour
+    const bool active = grp < wk.count;   // no early exit: every lane takes part in the shuffles
+    const SceneDev& S = scenes[wk.scene];
+    const int eid = active ? S.elems[wk.begin + grp] : 0;
     const int* tp = S.topo + (size_t)eid * NE;
     int vid[NI];
     float4 u[NI];
@@ -1532,24 +1532,21 @@ void vertex_mat(int mat, const SceneDev* scenes, const VWork* work, int n_work, 
 }
 
 template <int E, bool RAW>
-void xpbd_mat(int mat, const SceneDev* scenes, const int* elems, int begin, int count, int scene, const StepParams& P,
-              cudaStream_t st) {
-    constexpr int GPB = kBlock / XpbdLanes<E>::G;
-    const int grid = (count + GPB - 1) / GPB;
+void xpbd_mat(int mat, const SceneDev* scenes, const XWork* work, int n_work, const StepParams& P, cudaStream_t st) {
     switch (mat) {
-        case 0: launch_pdl(k_xpbd<E, 0, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
-        case 1: launch_pdl(k_xpbd<E, 1, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
-        case 2: launch_pdl(k_xpbd<E, 2, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
-        case 3: launch_pdl(k_xpbd<E, 3, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
-        case 4: launch_pdl(k_xpbd<E, 4, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
-        default: launch_pdl(k_xpbd<E, 5, RAW>, grid, kBlock, 0, st, scenes, elems, begin, count, scene, P); break;
+        case 0: launch_pdl(k_xpbd<E, 0, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
+        case 1: launch_pdl(k_xpbd<E, 1, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
+        case 2: launch_pdl(k_xpbd<E, 2, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
+        case 3: launch_pdl(k_xpbd<E, 3, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
+        case 4: launch_pdl(k_xpbd<E, 4, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
+        default: launch_pdl(k_xpbd<E, 5, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
     }
 }
 template <int E>
-void xpbd_form(int mat, bool raw, const SceneDev* scenes, const int* elems, int begin, int count, int scene,
-               const StepParams& P, cudaStream_t st) {
-    if (raw) xpbd_mat<E, true>(mat, scenes, elems, begin, count, scene, P, st);
-    else xpbd_mat<E, false>(mat, scenes, elems, begin, count, scene, P, st);
+void xpbd_form(int mat, bool raw, const SceneDev* scenes, const XWork* work, int n_work, const StepParams& P,
+               cudaStream_t st) {
+    if (raw) xpbd_mat<E, true>(mat, scenes, work, n_work, P, st);
+    else xpbd_mat<E, false>(mat, scenes, work, n_work, P, st);
 }
 }  // namespace
 
@@ -1650,10 +1647,10 @@ void launch_predict(const SceneDev* scenes, const NWork* work, int n_work, int k
     launch_pdl(k_predict, n_work, kNodeChunk, 0, st, scenes, work, n_work, kind, use_force, chebyshev, P);
 }
 
-void launch_velocity(const SceneDev* scenes, const NWork* work, int n_work, float global_damping, int pbd,
-                     const StepParams& P, cudaStream_t st) {
+void launch_velocity(const SceneDev* scenes, const NWork* work, int n_work, int pbd, const StepParams& P,
+                     cudaStream_t st) {
     if (n_work <= 0) return;
-    launch_pdl(k_velocity, n_work, kNodeChunk, 0, st, scenes, work, n_work, global_damping, pbd, P);
+    launch_pdl(k_velocity, n_work, kNodeChunk, 0, st, scenes, work, n_work, pbd, P);
 }
 
 void launch_chebyshev(const SceneDev* scenes, const NWork* work, int n_work, const StepParams& P, cudaStream_t st) {
@@ -1686,15 +1683,26 @@ void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, i
     launch_pdl(k_constraints, n_work, kNodeChunk, 0, st, scenes, work, n_work, box_pass);
 }
 
-void launch_xpbd(int element, int material, bool raw, const SceneDev* scenes, const int* elems, int begin, int count,
-                 int scene, const StepParams& P, cudaStream_t st) {
-    if (count <= 0) return;
+void launch_xpbd(int element, int material, bool raw, const SceneDev* scenes, const XWork* work, int n_work,
+                 const StepParams& P, cudaStream_t st) {
+    if (n_work <= 0) return;
     switch (element) {
-        case 3: xpbd_form<3>(material, false, scenes, elems, begin, count, scene, P, st); break;   // always V0
-        case 6: xpbd_form<6>(material, raw, scenes, elems, begin, count, scene, P, st); break;
-        case 7: xpbd_form<7>(material, raw, scenes, elems, begin, count, scene, P, st); break;
-        case 8: xpbd_form<8>(material, raw, scenes, elems, begin, count, scene, P, st); break;
-        case 9: xpbd_form<9>(material, raw, scenes, elems, begin, count, scene, P, st); break;
+        case 3: xpbd_form<3>(material, false, scenes, work, n_work, P, st); break;   // always V0
+        case 6: xpbd_form<6>(material, raw, scenes, work, n_work, P, st); break;
+        case 7: xpbd_form<7>(material, raw, scenes, work, n_work, P, st); break;
+        case 8: xpbd_form<8>(material, raw, scenes, work, n_work, P, st); break;
+        case 9: xpbd_form<9>(material, raw, scenes, work, n_work, P, st); break;
+    }
+}
+
+int xpbd_elements_per_block(int element) {
+    switch (element) {
+        case 3: return kBlock / XpbdLanes<3>::G;
+        case 6: return kBlock / XpbdLanes<6>::G;
+        case 7: return kBlock / XpbdLanes<7>::G;
+        case 8: return kBlock / XpbdLanes<8>::G;
+        case 9: return kBlock / XpbdLanes<9>::G;
+        default: return 1;
     }
 }
 

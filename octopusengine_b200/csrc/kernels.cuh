@@ -18,8 +18,9 @@ void launch_commit(const SceneDev* scenes, const VWork* work, int n_work, cudaSt
 // kind 0: VBD predictor, kind 1: semi-implicit Euler (use_force: add the force in u_new)
 void launch_predict(const SceneDev* scenes, const NWork* work, int n_work, int kind, int use_force, int chebyshev,
                     const StepParams& P, cudaStream_t st);
-void launch_velocity(const SceneDev* scenes, const NWork* work, int n_work, float global_damping, int pbd,
-                     const StepParams& P, cudaStream_t st);
+// pbd: the GPU_PBD velocity update with each scene's global damping
+void launch_velocity(const SceneDev* scenes, const NWork* work, int n_work, int pbd, const StepParams& P,
+                     cudaStream_t st);
 void launch_chebyshev(const SceneDev* scenes, const NWork* work, int n_work, const StepParams& P, cudaStream_t st);
 // box_pass 0: work indexes fixed-id chunks; 1: work indexes node chunks (box clamp)
 void launch_constraints(const SceneDev* scenes, const NWork* work, int n_work, int box_pass, cudaStream_t st);
@@ -36,9 +37,11 @@ void launch_wait_probe(int* error, long limit, cudaStream_t st);
 // One scripted effect of one scene (kind 0 crush / 1 random sphere over the node chunks in
 // work, kind 2 high stretch over its ids); a no-op while the effect is inactive.
 void launch_effect(const SceneDev* scene, const NWork* work, int n_work, int slot, int kind, float dt, cudaStream_t st);
-// raw: the kernel_XPBD_V1/V2 update form (ignored for Tetra4, which always uses V0)
-void launch_xpbd(int element, int material, bool raw, const SceneDev* scenes, const int* elems, int begin, int count,
-                 int scene, const StepParams& P, cudaStream_t st);
+// raw: the kernel_XPBD_V1/V2 update form (ignored for Tetra4, which always uses V0); one block
+// per work item (xpbd_elements_per_block elements of one scene's colour)
+void launch_xpbd(int element, int material, bool raw, const SceneDev* scenes, const XWork* work, int n_work,
+                 const StepParams& P, cudaStream_t st);
+int xpbd_elements_per_block(int element);
 // Per-element diagnostics of GPU_FEM (kind 0 stress, 1 volume, 2 volume change, 3 inverted,
 // 4 stress with the reference kernel's accumulated Jx).
 void launch_element_diag(int element, int material, const SceneDev* scenes, int scene, int n_elements, int kind, float* out,

@@ -176,6 +176,8 @@ struct oct_scene {
     int n_fwork = 0;
     int* d_elems = nullptr;         // XPBD: colour-sorted element ids
     std::vector<int> elem_off;
+    XWork* d_xwork = nullptr;       // XPBD: block work items of the scene's own steps
+    std::vector<int> xwork_off;     // per colour: [xwork_off[c], xwork_off[c+1])
     double* d_red = nullptr;        // 4 doubles of reduction scratch
     float* d_io = nullptr;          // n_nodes x 3 floats: node state in and out (allocated on first use)
     float* d_diag = nullptr;        // per-element diagnostics output (allocated on first use)
@@ -202,10 +204,12 @@ struct oct_batch {
     int* d_pending = nullptr;
     std::vector<int> pending_host;
     int* d_status = nullptr;        // SceneDev::status of each scene during the batch's frames
+    int solver = OCT_SOLVER_VBD;    // VBD or XPBD: a batch holds scenes of one solver
+    XWork* d_xwork = nullptr;       // XPBD: block items, per group and colour
     struct Group {
-        int element, material, tpv;
+        int element, material, tpv;     // XPBD: tpv holds the raw (V1/V2) update flag
         bool in_place;
-        std::vector<int> off;   // per colour, into the group's part of d_vwork
+        std::vector<int> off;   // per colour, into the group's part of d_vwork (XPBD: d_xwork)
         int base = 0;
         cudaStream_t stream = nullptr;
         cudaEvent_t done = nullptr;
@@ -269,6 +273,11 @@ void append_vwork(std::vector<VWork>& out, int scene, int begin, int end, int tp
 }
 void append_nwork(std::vector<NWork>& out, int scene, int n) {
     for (int s = 0; s < n; s += kNodeChunk) out.push_back({scene, s, std::min(kNodeChunk, n - s), 0});
+}
+
+// XPBD block items over [begin, end) of a scene's colour-sorted element list.
+void append_xwork(std::vector<XWork>& out, int scene, int begin, int end, int per_block) {
+    for (int e = begin; e < end; e += per_block) out.push_back({scene, e, std::min(per_block, end - e), 0});
 }
 
 // lanes per vertex chosen when the description leaves it at 0 (0 = packed pairs)
@@ -569,6 +578,13 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
         std::vector<int32_t> flat;
         for (auto& v : elems_by_color) { flat.insert(flat.end(), v.begin(), v.end()); s->elem_off.push_back((int)flat.size()); }
         if ((st = upload(c, s->mem, s->d_elems, flat))) return st;
+        std::vector<XWork> xw;
+        s->xwork_off.assign(1, 0);
+        for (int k = 0; k + 1 < (int)s->elem_off.size(); ++k) {
+            append_xwork(xw, 0, s->elem_off[k], s->elem_off[k + 1], xpbd_elements_per_block(d->element));
+            s->xwork_off.push_back((int)xw.size());
+        }
+        if ((st = upload(c, s->mem, s->d_xwork, xw))) return st;
         // VBD-style slots are unused; keep the identity order for the getters
         for (int i = 0; i < N; ++i) slot_vids.push_back(i);
         s->color_off = {0, N};
@@ -750,6 +766,8 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     for (int k = 0; k < kMaxEffects; ++k) { s->effects[k] = EffectDev{}; s->effects[k].kind = -1; }
     if ((st = upload(c, s->mem, s->d_effects, std::vector<EffectDev>(s->effects, s->effects + kMaxEffects)))) return st;
     h.effects = s->d_effects;
+    h.elems = s->d_elems;
+    h.global_damping = s->global_damping;
     if ((st = upload(c, s->mem, s->d_status, std::vector<int>{0}))) return st;
     h.status = s->d_status;
     s->topo_host.assign(d->topology, d->topology + (size_t)E * NE);
@@ -867,7 +885,7 @@ void vbd_substep(oct_scene* s, float dt) {
             c->launches++;
         }
     }
-    launch_velocity(s->d_scene, s->d_nwork, s->n_nwork, 0.f, 0, P, st);
+    launch_velocity(s->d_scene, s->d_nwork, s->n_nwork, 0, P, st);
     c->launches++;
 }
 
@@ -880,14 +898,14 @@ void xpbd_substep(oct_scene* s, float dt) {
     launch_predict(s->d_scene, s->d_nwork, s->n_nwork, 1, 0, 0, P, st);
     c->launches++;
     for (int k = 0; k < s->n_colors && s->xpbd_project; ++k) {
-        launch_xpbd(s->element, s->material, s->xpbd_raw, s->d_scene, s->d_elems, s->elem_off[k],
-                    s->elem_off[k + 1] - s->elem_off[k], 0, P, st);
+        launch_xpbd(s->element, s->material, s->xpbd_raw, s->d_scene, s->d_xwork + s->xwork_off[k],
+                    s->xwork_off[k + 1] - s->xwork_off[k], P, st);
         c->launches++;
     }
     if (s->n_fixed) { launch_constraints(s->d_scene, s->d_fwork, s->n_fwork, 0, st); c->launches++; }
     enqueue_effects(s, dt, st);
     if (s->box) { launch_constraints(s->d_scene, s->d_nwork, s->n_nwork, 1, st); c->launches++; }
-    launch_velocity(s->d_scene, s->d_nwork, s->n_nwork, s->global_damping, 1, P, st);
+    launch_velocity(s->d_scene, s->d_nwork, s->n_nwork, 1, P, st);
     c->launches++;
 }
 
@@ -1513,25 +1531,54 @@ oct_status oct_batch_create(oct_ctx* c, oct_scene* const* scenes, int n, oct_bat
     auto b = std::make_unique<oct_batch>();
     b->ctx = c;
     b->mem.ctx = c;
+    if (!scenes[0]) return OCT_EINVAL;
+    b->solver = scenes[0]->solver;
+    if (b->solver == OCT_SOLVER_EXPLICIT) return fail(c, OCT_ENOTSUP, "batches hold VBD or XPBD scenes");
+    const bool xpbd = b->solver == OCT_SOLVER_XPBD;
     b->iterations = scenes[0]->iterations;
     b->rho = scenes[0]->rho;
     std::vector<SceneDev> hs;
     std::vector<NWork> nw, fw, bw;
     std::map<std::pair<std::pair<int, int>, std::pair<int, int>>, int> gid;
     std::vector<std::vector<std::vector<VWork>>> gwork;   // group -> colour -> items
+    std::vector<std::vector<std::vector<XWork>>> gxwork;  // XPBD: group -> colour -> items
     size_t off = 0;
     for (int i = 0; i < n; ++i) {
         oct_scene* s = scenes[i];
         if (!s || s->ctx != c) return fail(c, OCT_EINVAL, "scene from another context");
-        if (s->solver != OCT_SOLVER_VBD) return fail(c, OCT_ENOTSUP, "batches hold VBD scenes");
-        if (s->iterations != b->iterations || s->rho != b->rho) return fail(c, OCT_ENOTSUP, "batch scenes need equal iterations and rho");
-        if (s->order_mode != OCT_ORDER_ASCENDING) return fail(c, OCT_ENOTSUP, "batches use the ascending colour order");
+        if (s->solver != b->solver) return fail(c, OCT_ENOTSUP, "a batch holds scenes of one solver");
+        if (!xpbd && (s->iterations != b->iterations || s->rho != b->rho))
+            return fail(c, OCT_ENOTSUP, "batch scenes need equal iterations and rho");
+        if (!xpbd && s->order_mode != OCT_ORDER_ASCENDING) return fail(c, OCT_ENOTSUP, "batches use the ascending colour order");
         if (s->mg_sub) return fail(c, OCT_ENOTSUP, "multigrid scenes are stepped alone");
         b->scenes.push_back(s);
         hs.push_back(s->h);
         b->pending_host.push_back(s->pending_host);
         b->state_off.push_back(off);
         off += (size_t)s->n_nodes * 6;
+        append_nwork(nw, i, s->n_nodes);
+        std::vector<NWork> f1;
+        append_nwork(f1, i, s->n_fixed);
+        fw.insert(fw.end(), f1.begin(), f1.end());
+        if (s->box) append_nwork(bw, i, s->n_nodes);
+        if (xpbd) {   // groups by (element, material, update form); scenes that project nothing add no work
+            if (!s->xpbd_project) continue;
+            auto key = std::make_pair(std::make_pair(s->element, s->material), std::make_pair(s->xpbd_raw ? 1 : 0, 0));
+            auto it = gid.find(key);
+            if (it == gid.end()) {
+                it = gid.emplace(key, (int)b->groups.size()).first;
+                oct_batch::Group g;
+                g.element = s->element; g.material = s->material; g.tpv = s->xpbd_raw ? 1 : 0; g.in_place = true;
+                b->groups.push_back(g);
+                gxwork.emplace_back();
+            }
+            auto& cw = gxwork[it->second];
+            const int nc = (int)s->elem_off.size() - 1;
+            if ((int)cw.size() < nc) cw.resize(nc);
+            for (int k = 0; k < nc; ++k)
+                append_xwork(cw[k], i, s->elem_off[k], s->elem_off[k + 1], xpbd_elements_per_block(s->element));
+            continue;
+        }
         auto key = std::make_pair(std::make_pair(s->element, s->material), std::make_pair(s->tpv, s->in_place ? 1 : 0));
         auto it = gid.find(key);
         if (it == gid.end()) {
@@ -1544,20 +1591,24 @@ oct_status oct_batch_create(oct_ctx* c, oct_scene* const* scenes, int n, oct_bat
         auto& cw = gwork[it->second];
         if ((int)cw.size() < s->n_colors) cw.resize(s->n_colors);
         for (int k = 0; k < s->n_colors; ++k) append_vwork(cw[k], i, s->color_off[k], s->color_off[k + 1], s->tpv, s->own_off);
-        append_nwork(nw, i, s->n_nodes);
-        std::vector<NWork> f1;
-        append_nwork(f1, i, s->n_fixed);
-        fw.insert(fw.end(), f1.begin(), f1.end());
-        if (s->box) append_nwork(bw, i, s->n_nodes);
     }
     b->state_off.push_back(off);
     std::vector<VWork> all;
+    std::vector<XWork> xall;
     for (size_t g = 0; g < b->groups.size(); ++g) {
-        b->groups[g].base = (int)all.size();
         b->groups[g].off.assign(1, 0);
-        for (auto& items : gwork[g]) {
-            all.insert(all.end(), items.begin(), items.end());
-            b->groups[g].off.push_back((int)(all.size() - b->groups[g].base));
+        if (xpbd) {
+            b->groups[g].base = (int)xall.size();
+            for (auto& items : gxwork[g]) {
+                xall.insert(xall.end(), items.begin(), items.end());
+                b->groups[g].off.push_back((int)(xall.size() - b->groups[g].base));
+            }
+        } else {
+            b->groups[g].base = (int)all.size();
+            for (auto& items : gwork[g]) {
+                all.insert(all.end(), items.begin(), items.end());
+                b->groups[g].off.push_back((int)(all.size() - b->groups[g].base));
+            }
         }
         OCT_CUDA(c, cudaStreamCreateWithFlags(&b->groups[g].stream, cudaStreamNonBlocking));
         OCT_CUDA(c, cudaEventCreateWithFlags(&b->groups[g].done, cudaEventDisableTiming));
@@ -1568,6 +1619,7 @@ oct_status oct_batch_create(oct_ctx* c, oct_scene* const* scenes, int n, oct_bat
     if ((st = upload(c, b->mem, b->d_status, std::vector<int>(b->scenes.size(), 0)))) { b->mem.release(); return st; }
     for (size_t i = 0; i < hs.size(); ++i) hs[i].status = b->d_status + i;
     if ((st = upload(c, b->mem, b->d_scenes, hs)) || (st = upload(c, b->mem, b->d_vwork, all)) ||
+        (st = upload(c, b->mem, b->d_xwork, xall)) ||
         (st = upload(c, b->mem, b->d_nwork, nw)) || (st = upload(c, b->mem, b->d_fwork, fw)) ||
         (st = upload(c, b->mem, b->d_bwork, bw)) || (st = upload(c, b->mem, b->d_pending, b->pending_host))) {
         b->mem.release();
@@ -1584,7 +1636,32 @@ oct_status oct_batch_create(oct_ctx* c, oct_scene* const* scenes, int n, oct_bat
 
 namespace {
 // Enqueue one sub-step of the whole batch on the context stream (captured into a graph).
+// One GPU_PBD::step (octopus/src/GPU/PBD/GPU_PBD.cu:20-26) over all scenes of an XPBD batch:
+// predictor, per colour one launch per (element type, material, update form) group with the
+// groups on parallel branches, constraints, velocity update with each scene's damping.
+void batch_substep_xpbd(oct_batch* b, float dt) {
+    oct_ctx* c = b->ctx;
+    cudaStream_t st = c->stream;
+    StepParams P = base_params(c, dt);
+    launch_predict(b->d_scenes, b->d_nwork, b->n_nwork, 1, 0, 0, P, st);
+    cudaEventRecord(b->fork, st);
+    for (auto& g : b->groups) {
+        cudaStreamWaitEvent(g.stream, b->fork, 0);
+        for (size_t k = 0; k + 1 < g.off.size(); ++k)
+            launch_xpbd(g.element, g.material, g.tpv != 0, b->d_scenes, b->d_xwork + g.base + g.off[k],
+                        g.off[k + 1] - g.off[k], P, g.stream);
+        cudaEventRecord(g.done, g.stream);
+        cudaStreamWaitEvent(st, g.done, 0);
+    }
+    if (b->n_fwork) launch_constraints(b->d_scenes, b->d_fwork, b->n_fwork, 0, st);
+    for (auto* s : b->scenes)
+        for (int k = 0; k < s->n_effects; ++k) launch_effect(s->d_scene, s->d_nwork, s->n_nwork, k, s->effects[k].kind, dt, st);
+    if (b->n_bwork) launch_constraints(b->d_scenes, b->d_bwork, b->n_bwork, 1, st);
+    launch_velocity(b->d_scenes, b->d_nwork, b->n_nwork, 1, P, st);
+}
+
 void batch_substep(oct_batch* b, float dt) {
+    if (b->solver == OCT_SOLVER_XPBD) { batch_substep_xpbd(b, dt); return; }
     oct_ctx* c = b->ctx;
     cudaStream_t st = c->stream;
     StepParams P = base_params(c, dt);
@@ -1620,11 +1697,19 @@ void batch_substep(oct_batch* b, float dt) {
             launch_chebyshev(b->d_scenes, b->d_nwork, b->n_nwork, P, st);
         }
     }
-    launch_velocity(b->d_scenes, b->d_nwork, b->n_nwork, 0.f, 0, P, st);
+    launch_velocity(b->d_scenes, b->d_nwork, b->n_nwork, 0, P, st);
 }
 
 uint64_t batch_launches_per_substep(const oct_batch* b) {
     uint64_t n = 2;
+    if (b->solver == OCT_SOLVER_XPBD) {
+        for (auto& g : b->groups)
+            for (size_t k = 0; k + 1 < g.off.size(); ++k) n += g.off[k + 1] > g.off[k] ? 1 : 0;
+        if (b->n_fwork) ++n;
+        if (b->n_bwork) ++n;
+        for (auto* s : b->scenes) n += (uint64_t)s->n_effects;
+        return n;
+    }
     for (auto& g : b->groups) n += (uint64_t)(g.off.size() - 1) * (g.in_place ? 1 : 2) * b->iterations;
     if (b->n_fwork) n += b->iterations;
     if (b->n_bwork) n += b->iterations;
@@ -1682,6 +1767,7 @@ oct_status oct_batch_destroy(oct_batch* b) {
 oct_status oct_batch_group_info(oct_batch* b, int g, int32_t* element, int32_t* material, double* flops, double* bytes,
                                 int32_t* launches, int64_t* vertices) {
     if (!b || g < 0 || g >= (int)b->groups.size()) return OCT_EINVAL;
+    if (b->solver != OCT_SOLVER_VBD) return OCT_ENOTSUP;
     const auto& G = b->groups[g];
     // Algorithmic work of one sweep: every free vertex of every scene of the group once.
     // flops: per (owner, quadrature point) term vbd_term_flops; bytes: per vertex u, u_last,
@@ -1710,6 +1796,7 @@ oct_status oct_batch_group_info(oct_batch* b, int g, int32_t* element, int32_t* 
 
 oct_status oct_batch_time_group(oct_batch* b, int g, int sweeps, float dt, float* ms) {
     if (!b || g < 0 || g >= (int)b->groups.size() || sweeps <= 0 || !ms || !(dt > 0.f)) return OCT_EINVAL;
+    if (b->solver != OCT_SOLVER_VBD) return OCT_ENOTSUP;
     oct_ctx* c = b->ctx;
     const auto& G = b->groups[g];
     StepParams P = base_params(c, dt);

@@ -120,3 +120,52 @@ def test_set_mapping_mid_run_matches_oracle(ctx, mapping):
         s.step(1 / 60, 2)
         o64.step(1 / 60, 2)
     assert rel_err(s.get_position(), o64.get(0)) < 1e-5
+
+
+def test_xpbd_batch_equals_scenes_alone_and_the_oracle(ctx):
+    """GPU_PBD::step over an XPBD batch (mixed element types, materials, update forms and
+    global damping, one launch per group and colour across the scenes) gives each scene's own
+    result bit for bit (the elements of a colour share no node, so their order does not
+    matter), and matches the oracle."""
+    import octopusengine_b200 as ob
+    rng = np.random.default_rng(5)
+    cases = [(O.TETRA, O.STABLE_NEOHOOKE, O.XPBD_OPTISHARED, 0.0), (O.TETRA10, O.NEOHOOKE, O.XPBD_OPTISHARED, 0.5),
+             (O.HEXA, O.STVK, O.XPBD_V0, 0.2), (O.TETRA10, O.COROTATED, O.XPBD_V0, 0.0),
+             (O.HEXA27, O.STABLE_NEOHOOKE, O.XPBD_QUADRATURE, 1.0), (O.HEXA, O.STABLE_NEOHOOKE, O.XPBD_OPTIGROUP, 0.0),
+             (O.TETRA, O.HOOKE, O.XPBD_OPTISHARED, 0.3)]
+    alone, mixed, oracles = [], [], []
+    for e, mat, ver, damp in cases:
+        cells = (2, 1, 1) if e == O.HEXA27 else (int(rng.integers(2, 5)), 2, int(rng.integers(1, 3)))
+        s, o32, o64, mesh = pair(ctx, e, cells=cells, material=mat, solver="xpbd", young=1e5, xpbd_version=ver,
+                                 global_damping=damp)
+        t, _, _, _ = pair(ctx, e, cells=cells, material=mat, solver="xpbd", young=1e5, xpbd_version=ver,
+                          global_damping=damp)
+        alone.append(s)
+        mixed.append(t)
+        oracles.append(o32)
+    batch = ob.Batch(ctx, mixed)
+    for frame in range(3):
+        for s in alone:
+            s.step(1 / 60, 5)
+        batch.step(1 / 60, 5)
+        if frame == 0:   # after one frame within the FP32 parity bar of the XPBD tests
+            for o, b in zip(oracles, mixed):
+                o.step(1 / 60, 5)
+                assert rel_err(b.get_position(), o.get(0)) < 1e-5
+    assert (batch.status() == 0).all()
+    for a, b in zip(alone, mixed):
+        np.testing.assert_array_equal(b.get_position(), a.get_position())
+        np.testing.assert_array_equal(b.get_velocity(), a.get_velocity())
+    batch.close()
+
+
+def test_batches_hold_one_solver(ctx):
+    import octopusengine_b200 as ob
+    a, _, _, _ = pair(ctx, O.TETRA, cells=(2, 1, 1), solver="xpbd")
+    b, _, _, _ = pair(ctx, O.TETRA, cells=(2, 1, 1))
+    c, _, _, _ = pair(ctx, O.TETRA, cells=(2, 1, 1), solver="explicit")
+    with pytest.raises(ob.OctError) as e:
+        ob.Batch(ctx, [a, b])
+    assert e.value.status == 6   # OCT_ENOTSUP
+    with pytest.raises(ob.OctError):
+        ob.Batch(ctx, [c])
