@@ -12,7 +12,13 @@ metric: vertex-iterations/s = sum over scenes of free nodes x iterations x sub-s
 step, / time.  Also reported: the plain single-scene drop-in path (each scene stepped on
 its own, FP32, one launch per colour, no graph) on the same scenes and GPU, p50/p99 step
 latency, the end-to-end number through the C ABI with host buffers, the roofline of the
-dominant kernel, and the reference CPU VBD path timed on the host cores.
+dominant kernel (SURVEY 8(d) algorithmic flops and bytes; the executed-flop rate beside
+them), the reference CPU VBD path timed on the host cores (one thread, as the reference runs;
+all threads as an extension), the timed run's error against the FP64 oracle on a sample of
+its scenes (`parity`), and, on the same GPU, config 2 as a single scene (`p2_single`), the
+same 256 beams as XPBD scenes in one batch (`xpbd_batched`, element-projections/s) and a
+15 s Poisson request stream at 4 requests/s through the request loop (`served`, p50/p99
+frame and request latency).  --no-extra skips the last three, --no-cpu the CPU legs.
 
 Single-scene solver workloads of the P2 beam (64x16x16 hex grid x 6 tets = 98,304 P2 elements,
 140,481 nodes, E=1e6, nu=0.49, rho=1100, x = 0 fixed, v0 ~ N(0, 0.05) from the seed):
@@ -31,6 +37,7 @@ and the plain single-scene path on a sample of the same requests.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                     [--workload batched|p2|cfg1|cube_p3|cube_q2|xpbd_p2|explicit_p2|served]
+                    [--scenes N] [--no-plain] [--no-cpu] [--no-extra]
 """
 import argparse
 import concurrent.futures as cf
