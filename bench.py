@@ -15,10 +15,11 @@ latency, the end-to-end number through the C ABI with host buffers, the roofline
 dominant kernel (SURVEY 8(d) algorithmic flops and bytes; the executed-flop rate beside
 them), the reference CPU VBD path timed on the host cores (one thread, as the reference runs;
 all threads as an extension), the timed run's error against the FP64 oracle on a sample of
-its scenes (`parity`), and, on the same GPU, config 2 as a single scene (`p2_single`), the
-same 256 beams as XPBD scenes in one batch (`xpbd_batched`, element-projections/s) and a
+its scenes (`parity`), and, on the same GPU, config 2 as a single scene (`p2_single`), config
+3's P3 and Q2 cubes at 32^3 cells (`cube`), the same 256 beams as XPBD scenes in one batch
+(`xpbd_batched`, element-projections/s) and a
 15 s Poisson request stream at 4 requests/s through the request loop (`served`, p50/p99
-frame and request latency).  --no-extra skips the last three, --no-cpu the CPU legs.
+frame and request latency).  --no-extra skips the last four, --no-cpu the CPU legs.
 
 Single-scene solver workloads of the P2 beam (64x16x16 hex grid x 6 tets = 98,304 P2 elements,
 140,481 nodes, E=1e6, nu=0.49, rho=1100, x = 0 fixed, v0 ~ N(0, 0.05) from the seed):
@@ -507,6 +508,44 @@ def single_scene_p2(ctx, seed, stream, warmup=3, steps=5):
     return out
 
 
+def single_cube(ctx, name, seed, stream, warmup=3, steps=3):
+    """Config 3 at full size: the 1 m cube of 32^3 cells as P3 (912,673 nodes) or Q2 (274,625
+    nodes), per-element Young modulus, bottom fixed and top moved down 20 % over 50 frames;
+    2 sub-steps x 10 iterations per 1/60 s frame, mixed precision, autotuned mapping."""
+    import torch
+    import octopusengine_b200 as ob
+    specs, iterations, substeps, frame_dt = workload_specs(name, seed)
+    t0 = time.time()
+    sc = build_scene(ctx, specs[0], iterations, ob.PREC_MIXED, seed)
+    setup_s = time.time() - t0
+    mapping = ob.autotune_mapping(ctx, [sc], frame_dt / substeps, sweeps=2)
+    b = ob.Batch(ctx, [sc])
+    frame = [0]
+
+    def step():
+        frame[0] += 1
+        sc.set_fixation((0.0, 0.0, -0.2 * min(frame[0], 50) / 50.0), group=1)
+        b.step(frame_dt, substeps)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    vit = (sc.n_nodes - sc.n_fixed) * iterations * substeps
+    out = {"value": vit / (ms * 1e-3), "unit": "vertex-iter/s", "ms_per_frame": ms, "frames": steps,
+           "nodes": sc.n_nodes, "elements": sc.n_elements, "mapping": mapping.get(specs[0]["element"]),
+           "setup_s": setup_s, "status": int(b.status()[0])}
+    b.close()
+    sc.close()
+    return out
+
+
 def batched_xpbd(ctx, specs, seed, stream, threads, warmup=3, steps=5, substeps=5, frame_dt=FRAME_DT):
     """The batched workload's scenes as XPBD scenes (reference default OptiShared: V0 for P1, the
     raw V2 update for P2/Q1) in one batch: per 1/60 s frame 5 sub-steps of GPU_PBD::step over
@@ -915,9 +954,10 @@ def main():
                  "path": "each scene stepped alone through oct_scene_step: FP32, one launch per colour, no graph"}
 
     # ---- the rest of the metric on the same GPU: config 2 alone, and a short served stream
-    p2_line, served_line, xpbd_line = None, None, None
+    p2_line, served_line, xpbd_line, cube_lines = None, None, None, None
     if rank == 0 and world == 1 and args.workload == "batched" and not args.no_extra:
         p2_line = single_scene_p2(ctx, args.seed, stream)
+        cube_lines = {w: single_cube(ctx, w, args.seed, stream) for w in ("cube_p3", "cube_q2")}
         xpbd_line = batched_xpbd(ctx, specs, args.seed, stream, threads)
         served_line = served_stream(ctx, args.serve_rate, args.serve_window, args.seed, threads)
 
@@ -963,6 +1003,7 @@ def main():
             "cpu_baseline": cpu,
             "parity": parity,
             "p2_single": p2_line,
+            "cube": cube_lines,
             "xpbd_batched": xpbd_line,
             "served": served_line,
             "setup_s": setup_s,

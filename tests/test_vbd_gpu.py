@@ -61,13 +61,23 @@ def test_energy_trace_100_steps_config1(ctx):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-def test_mixed_precision_closer_to_fp64(ctx, precision):
+def test_both_precisions_closer_to_fp64_than_the_fp32_restatement(ctx, precision):
+    """Three frames of a nearly incompressible P2 beam (nu = 0.49, 5 sub-steps x 10 iterations):
+    plain FP32 and mixed precision both stay closer to the FP64 oracle than the FP32 oracle
+    does (the product forms F from the displacement).  Mixed precision is not measurably
+    closer than plain at this size; its compensated sums and FP64 solves guard blocks these
+    scenes do not reach."""
     s, o32, o64, mesh = pair(ctx, O.TETRA10, cells=(6, 2, 2), size=(2.0, 0.5, 0.5), iterations=10, young=1e6,
                              poisson=0.49, density=1100.0, precision=precision)
     for _ in range(3):
         s.step(1 / 60, 5)
+        o32.step(1 / 60, 5)
         o64.step(1 / 60, 5)
-    assert disp_err(s.get_position(), o64.get(0), mesh["X"]) < 1e-2
+    ref = o64.get(0)
+    e = disp_err(s.get_position(), ref, mesh["X"])
+    e32 = disp_err(o32.get(0), ref, mesh["X"])
+    assert e <= e32 + 1e-6, (e, e32)
+    assert e < 1e-3
 
 
 def test_jacobi_colour_reduction_matches_oracle(ctx):
