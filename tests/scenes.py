@@ -59,3 +59,19 @@ def disp_err(a, b, X):
     """max-norm error relative to the max-norm of the reference displacement."""
     d = np.asarray(b) - X
     return float(np.abs(np.asarray(a, np.float64) - b).max() / max(np.abs(d).max(), 1e-30))
+
+
+def check_parity(p, o32, o64, X, label="", factor=3.0):
+    """The parity bar of the GPU tests, on both scales: positions within 1e-5 of the position
+    magnitude against the FP64 oracle, and the error relative to the step's displacement at
+    most `factor` times the FP32 oracle's own (plus the FP32 rounding of the positions, which
+    bounds what any FP32 state can resolve).  Returns (product error, FP32 oracle error) on the
+    displacement scale."""
+    ref = o64.get(0)
+    assert rel_err(p, ref) < 1e-5, (label, rel_err(p, ref))
+    d = np.abs(np.asarray(ref) - X).max()
+    floor = 2.0 * np.finfo(np.float32).eps * np.abs(ref).max() / max(d, 1e-30)
+    e = disp_err(p, ref, X)
+    e32 = disp_err(o32.get(0), ref, X)
+    assert e <= factor * e32 + floor, (label, e, e32, floor)
+    return e, e32

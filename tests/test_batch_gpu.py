@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import oracle_lib as O
-from scenes import pair, rel_err
+from scenes import check_parity, pair, rel_err
 
 pytestmark = pytest.mark.gpu
 
@@ -38,8 +38,8 @@ def test_batch_equals_single_scenes(ctx):
             s.step(1 / 60, 4)
         batch.step(1 / 60, 4)
     for a, b in zip(alone, mixed):
-        pa, pb = a.get_position(), b.get_position()
-        assert rel_err(pb, pa) < 1e-6, rel_err(pb, pa)
+        # the same kernels over the same work items: a batch gives each scene its own result
+        np.testing.assert_array_equal(b.get_position(), a.get_position())
     for s in alone + mixed:
         s.close()
     batch.close()
@@ -51,10 +51,10 @@ def test_batch_matches_oracle_and_state_round_trip(ctx):
     s2, p32, p64, mesh2 = pair(ctx, O.HEXA, cells=(3, 2, 2), iterations=6)
     batch = ob.Batch(ctx, [s1, s2])
     batch.step(1 / 60, 3)
-    o64.step(1 / 60, 3)
-    p64.step(1 / 60, 3)
-    assert rel_err(s1.get_position(), o64.get(0)) < 1e-5
-    assert rel_err(s2.get_position(), p64.get(0)) < 1e-5
+    for o in (o32, o64, p32, p64):
+        o.step(1 / 60, 3)
+    check_parity(s1.get_position(), o32, o64, mesh["X"], "P2 in a batch")
+    check_parity(s2.get_position(), p32, p64, mesh2["X"], "Q1 in a batch")
     state = np.zeros(batch.state_size, np.float32)
     batch.get_state(state)
     n1 = s1.n_nodes

@@ -5,12 +5,20 @@ import numpy as np
 import pytest
 
 import oracle_lib as O
-from scenes import pair, rel_err
+from scenes import check_parity, pair, rel_err
 
 pytestmark = pytest.mark.gpu
 
 
 XPBD_MATERIALS = [O.STABLE_NEOHOOKE, O.NEOHOOKE, O.STVK, O.HOOKE, O.COROTATED, O.FIXED_COROTATED]
+
+
+def s_rest(s):
+    import ctypes as C
+    from octopusengine_b200 import capi
+    X = np.zeros((s.n_nodes, 3), np.float32)
+    capi.check(capi.lib().oct_scene_get_rest_positions(s.handle, capi.ptr(X, C.c_float)), "rest positions")
+    return X
 
 
 def _run_xpbd(s, o32, o64, frames):
@@ -24,6 +32,7 @@ def _run_xpbd(s, o32, o64, frames):
         p = s.get_position()
         if k == 0:
             assert rel_err(p, o32.get(0)) < 1e-5
+            check_parity(p, o32, o64, s_rest(s), "xpbd first frame")
         ref32 = rel_err(o32.get(0), o64.get(0))
         e64 = rel_err(p, o64.get(0))
         assert e64 < max(1e-5, 2.0 * ref32), (k, e64, ref32)
@@ -80,7 +89,9 @@ def test_explicit_parity(ctx, element):
     for _ in range(5):
         s.step(1e-3, 20)
         o32.step(1e-3, 20)
+        o64.step(1e-3, 20)
     assert rel_err(s.get_position(), o32.get(0)) < 1e-5
+    check_parity(s.get_position(), o32, o64, mesh["X"], ("explicit", element))
     v = s.get_velocity()
     assert np.abs(v - o32.get(1)).max() < 1e-3 * max(1.0, np.abs(o32.get(1)).max())
 
