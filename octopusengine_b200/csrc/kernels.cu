@@ -188,7 +188,12 @@ __device__ __forceinline__ void kadd(float& s, float& c, float v) {
 // plain sum over its quadrature points, instead of once per point: the many-point elements
 // (P3 11 points, Q2 27), where the per-point compensation is a long dependent chain (sweep
 // rate measured +5 % P3, +32 % Q2; per point stays faster for P1, Q1 and P2).
-template <int E> struct CompensatePerElement { static constexpr bool value = E == 8 || E == 9; };
+#ifndef OCTB_COMPENSATE_PER_ELEMENT_EXTRA
+#define OCTB_COMPENSATE_PER_ELEMENT_EXTRA 0   // bit E: also compensate per element for element type E
+#endif
+template <int E> struct CompensatePerElement {
+    static constexpr bool value = E == 8 || E == 9 || ((OCTB_COMPENSATE_PER_ELEMENT_EXTRA >> E) & 1);
+};
 
 // Contribution of one quadrature point: f (3) and the symmetric H (6: 00 01 02 11 12 22).
 template <int MAT>
