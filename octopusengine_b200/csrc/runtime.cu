@@ -1486,7 +1486,10 @@ oct_status oct_batch_status(oct_batch* b, int32_t* out) {
     OCT_CUDA(c, cudaMemset(b->d_status, 0, sizeof(int) * n));
     int e = 0;   // context word: a time-out outside any one scene's work (constant-table staging)
     OCT_CUDA(c, cudaMemcpy(&e, c->d_error, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e & 1) OCT_CUDA(c, cudaMemset(c->d_error, 0, sizeof(int)));
+    if (e & 1) {   // taken over by the per-scene statuses; the other bits stay for their own checks
+        const int rest = e & ~1;
+        OCT_CUDA(c, cudaMemcpy(c->d_error, &rest, sizeof(int), cudaMemcpyHostToDevice));
+    }
     for (size_t i = 0; i < n; ++i)
         out[i] = (f[i] & kStatusNonFinite) ? OCT_ENUMERIC : ((f[i] & kStatusTimeout) || (e & 1)) ? OCT_ETIMEDOUT : OCT_OK;
     return OCT_OK;
