@@ -2,7 +2,8 @@
 
 * Config 2 at full size: the P2 beam of 64 x 16 x 16 cells (98,304 tet10, 140,481 nodes),
   E = 1e6, nu = 0.49, rho = 1100, x = 0 face fixed, v0 ~ N(0, 0.05) from the seed; one VBD
-  sub-step of 1/300 s with 10 iterations, in the drop-in (plain) and the mixed precision.
+  sub-step of 1/300 s with 10 iterations, in the drop-in (plain) and the mixed precision; one
+  XPBD frame of 5 sub-steps; 10 explicit steps of 1e-5 s.
 * Config 3 at 16^3 cells: the 1 m cube of P3 (117,649 nodes) and of Q2 (35,937 nodes) with a
   per-element Young modulus log-uniform in [1e4, 1e6], bottom fixed, top moved down by the
   first of 50 increments of 20 %; one frame of 2 sub-steps x 10 iterations.
@@ -146,3 +147,34 @@ def test_config4_sample_batched_mixed_autotuned(ctx):
         print("config 4 scene e%d n%d mapping %d: mixed %.3e, fp32 oracle %.3e" % (e, len(X), s.mapping(), got, e32))
         assert got <= 1.0 * e32 + ORACLE_FLOOR, (e, len(X), got, e32)
     b.close()
+
+
+@pytest.mark.parametrize("solver", ["xpbd", "explicit"])
+def test_config2_full_size_xpbd_and_explicit(ctx, solver):
+    """Config 2's other two solvers at full size (98,304 P2 elements, 140,481 nodes): one XPBD
+    frame of 5 sub-steps (1/60 s, the reference default OptiShared form), or 10 explicit
+    symplectic-Euler steps of 1e-5 s, against the FP64 oracle with the FP32 oracle's error as
+    the bar."""
+    import octopusengine_b200 as ob
+    X, T = ob.beam_mesh(ob.TETRA10, (64, 16, 16), (4.0, 1.0, 1.0))
+    fixed = ob.fixed_by_plane(X, (0.01, 0.0, 0.0), (-1.0, 0.0, 0.0))
+    m = ob.lumped_masses(ob.TETRA10, X, T, 1100.0, ob.MASS_FEMSHAPE)
+    v0 = np.random.default_rng(2024).normal(0, 0.05, X.shape).astype(np.float32)
+    kind = {"xpbd": ob.SOLVER_XPBD, "explicit": ob.SOLVER_EXPLICIT}[solver]
+    frame, n = (1.0 / 60.0, 5) if solver == "xpbd" else (1e-4, 10)
+    s = ob.Scene(ctx, ob.TETRA10, X, T, solver=kind, masses=m, fixed_ids=fixed, initial_velocity=v0,
+                 material=ob.STABLE_NEOHOOKE, young=1e6, poisson=0.49, gravity=(0.0, 0.0, -9.81))
+    s.step(frame, n)
+    got = s.get_position()
+    s.close()
+    out = []
+    for fp64 in (False, True):
+        sc = O.Scene(O.TETRA10, X, T, m, material=O.STABLE_NEOHOOKE, young=1e6, poisson=0.49,
+                     gravity=(0.0, 0.0, -9.81), fixed=fixed, v0=v0)
+        o = O.Solver(solver, sc, fp64=fp64)
+        o.step(frame, n)
+        out.append(o.get(0))
+    e = disp_err(got, out[1], X)
+    e32 = disp_err(out[0], out[1], X)
+    print("config 2 %s: product %.3e, fp32 oracle %.3e" % (solver, e, e32))
+    assert e <= 3.0 * e32 + ORACLE_FLOOR, (solver, e, e32)
