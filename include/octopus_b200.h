@@ -246,9 +246,10 @@ oct_status oct_scene_set_mapping(oct_scene* s, int threads_per_vertex);
 /* The mapping in effect: -1 packed pairs, else lanes per vertex (the measured default and the
  * fallback for vertices with more than 32 owners resolved); 0 for XPBD scenes. */
 oct_status oct_scene_get_mapping(oct_scene* s, int32_t* threads_per_vertex);
-/* Mapping autotuner (new): for each element type among the scenes, times one colour sweep of
- * all its scenes under every candidate mapping (packed pairs, 1, 2, 4, 8, 16, 32 lanes per
- * vertex) and sets the fastest on those scenes.  The timed sweeps write only the Jacobi
+/* Mapping autotuner (new): for each element type among the VBD and explicit scenes (XPBD
+ * scenes are skipped), times one colour sweep of all its scenes under every candidate mapping
+ * (packed pairs when every scene has owner entries and at most 32 owners per vertex, 1, 2, 4,
+ * 8, 16, 32 lanes per vertex) and sets the fastest on those scenes.  The timed sweeps write only the Jacobi
  * scratch buffer, so positions and velocities are unchanged.  chosen (may be NULL): per
  * element id the mapping picked (-1 packed), 0 for element types absent.  Run it before
  * oct_batch_create; it leaves no batch behind. */
@@ -415,13 +416,15 @@ oct_status oct_ctx_wait_probe(oct_ctx* ctx, int32_t limit);
 oct_status oct_ctx_stream(oct_ctx* ctx, void** stream);
 /* Measured FP32 FMA throughput of the device (TFLOP/s) from a register-resident FMA loop. */
 oct_status oct_fp32_peak(oct_ctx* ctx, double* tflops);
-/* Per element group g of a batch (scenes sharing element type, material and thread
- * mapping): algorithmic FP32 flops and minimal DRAM bytes of one VBD colour sweep (all
- * colours once), its launch count and vertex updates.  Returns OCT_EINVAL past the last group. */
+/* Per element group g of a VBD batch (scenes sharing element type, material and thread
+ * mapping): the FP32 flops the colour kernel executes and the minimal DRAM bytes of one VBD
+ * colour sweep (all colours once), its launch count and vertex updates.  Returns OCT_EINVAL
+ * past the last group, OCT_ENOTSUP for an XPBD batch. */
 oct_status oct_batch_group_info(oct_batch* b, int g, int32_t* element, int32_t* material, double* flops_per_sweep,
                                 double* bytes_per_sweep, int32_t* launches_per_sweep, int64_t* vertices_per_sweep);
-/* Runs `sweeps` colour sweeps of group g alone on the context stream (outside the graph,
- * state advances as in an iteration) and returns their total device time (CUDA events). */
+/* Runs `sweeps` colour sweeps of group g of a VBD batch alone on the context stream (outside
+ * the graph, state advances as in an iteration) and returns their total device time (CUDA
+ * events); OCT_ENOTSUP for an XPBD batch. */
 oct_status oct_batch_time_group(oct_batch* b, int g, int sweeps, float dt, float* ms);
 
 /* Allocation-free FP64 elastic energy (no counterpart entry point in the reference; its CPU
