@@ -773,7 +773,9 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     s->topo_host.assign(d->topology, d->topology + (size_t)E * NE);
     if ((st = s->mem.alloc(s->d_scene, 1))) return st;
     OCT_CUDA(c, cudaMemcpy(s->d_scene, &h, sizeof(SceneDev), cudaMemcpyHostToDevice));
-    s->pending_host = s->has_v0 ? 1 : 0;
+    // VBD moves by its implicit velocity, so an initial velocity waits for the first sub-step's
+    // predictor; XPBD and explicit step the velocity array itself, which already holds it
+    s->pending_host = s->has_v0 && d->solver == OCT_SOLVER_VBD ? 1 : 0;
     if ((st = upload(c, s->mem, s->d_pending, std::vector<int>{s->pending_host}))) return st;
     if ((st = s->mem.alloc(s->d_red, 4))) return st;
 
@@ -1748,9 +1750,14 @@ oct_status oct_batch_step(oct_batch* b, float frame_dt, int substeps) {
         c->launches += batch_launches_per_substep(b);
     }
     cudaEventRecord(c->ev1, c->stream);
-    for (auto* s : b->scenes) {   // the batch applied them; the scenes' own flags go too
-        if (s->pending_host) cudaMemsetAsync(s->d_pending, 0, sizeof(int), c->stream);
+    for (size_t i = 0; i < b->scenes.size(); ++i) {
+        // the batch applied the flags it took at creation; those scenes' own flags go too (a
+        // flag set on a scene after the batch was created stays for the scene's own next step)
+        if (!b->pending_host[i]) continue;
+        oct_scene* s = b->scenes[i];
+        cudaMemsetAsync(s->d_pending, 0, sizeof(int), c->stream);
         s->pending_host = 0;
+        b->pending_host[i] = 0;
     }
     return OCT_OK;
 }
