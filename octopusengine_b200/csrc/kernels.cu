@@ -1391,6 +1391,191 @@ __device__ __forceinline__ void dinv(D3 c0, D3 c1, D3 c2, D3& i0, D3& i1, D3& i2
     i0 = D3{r0.x, r1.x, r2.x} * id; i1 = D3{r0.y, r1.y, r2.y} * id; i2 = D3{r0.z, r1.z, r2.z} * id;
 }
 
+// ------------------------------------------------------------------------ explicit force
+// Element-centric force pass of the explicit integrator (the terms of kernel_fem_eval_force,
+// octopus/src/GPU/Explicit/GPU_FEM_Explicit.cu:5-64: f_i = sum_q -V P g_iq, minus k_d (sum_q
+// H_iq) v_i).  The explicit step has no colour order, so each element's deformation gradient
+// is formed once per quadrature point instead of once per (node, point) as in the vertex
+// kernel, and its nodes are gathered once instead of once per owner.  G lanes per element (as
+// k_xpbd): lane i gathers node i, lane q forms F at point q into shared memory, then lane i
+// evaluates its nodes' terms (material_terms, the arithmetic of the vertex kernel) at every
+// point and writes its per-(element, local node) force to `contrib`; k_explicit_gather sums
+// each node's owners in owner order.  Deterministic (no atomics).
+// P~ = V P JX_inv^T (columns T0 T1 T2) of the first Piola-Kirchhoff stress of material_terms'
+// materials, so that -V P g = -(T0 dN_0 + T1 dN_1 + T2 dN_2) for g = JX_inv^T dN.
+template <int MAT>
+__device__ __forceinline__ void pk1_tilde(V3 F0, V3 F1, V3 F2, float lam, float mu, float V, V3 m0, V3 m1, V3 m2,
+                                          V3& T0, V3& T1, V3& T2) {
+    V3 P0, P1, P2;   // columns of P
+    if (MAT == 2 || MAT == 3) {   // P = mu F + s cof(F)
+        const V3 C0 = cross(F1, F2), C1 = cross(F2, F0), C2 = cross(F0, F1);
+        const float J = dot(F0, C0);
+        const float sc = MAT == 3 ? lam * (J - 1.f) - mu : lam * (J - 1.f);
+        P0 = F0 * mu + C0 * sc; P1 = F1 * mu + C1 * sc; P2 = F2 * mu + C2 * sc;
+    } else if (MAT == 0) {        // P = lambda tr(E) I + mu E, E = (F + F^T)/2 - I
+        const float trE = F0.x + F1.y + F2.z - 3.f;
+        // E column c, row r: (F_rc + F_cr)/2 - d_rc, F_rc = row r of column c
+        const V3 E0 = mk(F0.x - 1.f, 0.5f * (F0.y + F1.x), 0.5f * (F0.z + F2.x));
+        const V3 E1 = mk(0.5f * (F1.x + F0.y), F1.y - 1.f, 0.5f * (F1.z + F2.y));
+        const V3 E2 = mk(0.5f * (F2.x + F0.z), 0.5f * (F2.y + F1.z), F2.z - 1.f);
+        const float lt = lam * trE;
+        P0 = E0 * mu + mk(lt, 0.f, 0.f); P1 = E1 * mu + mk(0.f, lt, 0.f); P2 = E2 * mu + mk(0.f, 0.f, lt);
+    } else {                      // StVK: P = lambda tr(E) F + 2 mu F E, E = (F^T F - I)/2
+        const float f00 = dot(F0, F0), f01 = dot(F0, F1), f02 = dot(F0, F2);
+        const float f11 = dot(F1, F1), f12 = dot(F1, F2), f22 = dot(F2, F2);
+        const float trE = 0.5f * (f00 + f11 + f22 - 3.f);
+        // column c of F E = sum_k F_k E_kc
+        const V3 FE0 = F0 * (0.5f * (f00 - 1.f)) + F1 * (0.5f * f01) + F2 * (0.5f * f02);
+        const V3 FE1 = F0 * (0.5f * f01) + F1 * (0.5f * (f11 - 1.f)) + F2 * (0.5f * f12);
+        const V3 FE2 = F0 * (0.5f * f02) + F1 * (0.5f * f12) + F2 * (0.5f * (f22 - 1.f));
+        const float lt = lam * trE, tm = 2.f * mu;
+        P0 = F0 * lt + FE0 * tm; P1 = F1 * lt + FE1 * tm; P2 = F2 * lt + FE2 * tm;
+    }
+    // column j of P JX_inv^T = sum_k P_k (m_k)_j
+    T0 = (P0 * m0.x + P1 * m1.x + P2 * m2.x) * V;
+    T1 = (P0 * m0.y + P1 * m1.y + P2 * m2.y) * V;
+    T2 = (P0 * m0.z + P1 * m1.z + P2 * m2.z) * V;
+}
+
+template <int E, int MAT>
+__global__ void __launch_bounds__(kBlock) k_explicit_elem(const SceneDev* __restrict__ scenes, int n_elements,
+                                                          float4* __restrict__ contrib, StepParams P) {
+    constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ, G = XpbdLanes<E>::G, GPB = kBlock / G;
+    constexpr int NI = (NE + G - 1) / G;   // nodes per lane
+    static_assert(NQ <= G, "one quadrature point per lane");
+    __shared__ __align__(16) float s_dN[((NQ * NE * 3 + 3) / 4) * 4];
+    __shared__ __align__(16) float4 s_u[GPB][NE];
+    __shared__ __align__(16) float4 s_F[GPB][NQ][3];   // F columns at each point
+    __shared__ __align__(16) float4 s_R[GPB][NQ][3];   // JX_inv columns, then (., V w_q, lambda, mu)
+    __shared__ unsigned long long s_mbar;
+    pdl_trigger();
+    stage_table(s_dN, gdN<E>(), NQ * NE * 3, &s_mbar, P.error);
+    pdl_wait();
+    const SceneDev& S = scenes[0];
+    const int lane = threadIdx.x % G, grp = threadIdx.x / G;
+    const int eid = blockIdx.x * GPB + grp;
+    const bool active = eid < n_elements;   // no early exit: the group synchronises with __syncwarp
+    const int* tp = S.topo + (size_t)(active ? eid : 0) * NE;
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+        const int i = lane + k * G;
+        if (active && i < NE) s_u[grp][i] = S.u[tp[i]];
+    }
+    __syncwarp();
+    if (active && lane < NQ) {
+        const int q = lane;
+        const float4* rec = S.eq + ((size_t)eid * S.eq_stride + (S.eq_stride == 1 ? 0 : q)) * 3;
+        const float4 A = rec[0], B = rec[1], C = rec[2];
+        const V3 m0 = mk(A.x, A.y, A.z), m1 = mk(A.w, B.x, B.y), m2 = mk(B.z, B.w, C.x);
+        V3 J0 = mk(0, 0, 0), J1 = J0, J2 = J0;
+#pragma unroll
+        for (int i = 0; i < NE; ++i) {
+            const float4 uu = s_u[grp][i];
+            const float* d = &s_dN[(q * NE + i) * 3];
+            J0.x = fmaf(uu.x, d[0], J0.x); J0.y = fmaf(uu.y, d[0], J0.y); J0.z = fmaf(uu.z, d[0], J0.z);
+            J1.x = fmaf(uu.x, d[1], J1.x); J1.y = fmaf(uu.y, d[1], J1.y); J1.z = fmaf(uu.z, d[1], J1.z);
+            J2.x = fmaf(uu.x, d[2], J2.x); J2.y = fmaf(uu.y, d[2], J2.y); J2.z = fmaf(uu.z, d[2], J2.z);
+        }
+        V3 F0 = J0 * m0.x + J1 * m0.y + J2 * m0.z;
+        V3 F1 = J0 * m1.x + J1 * m1.y + J2 * m1.z;
+        V3 F2 = J0 * m2.x + J1 * m2.y + J2 * m2.z;
+        F0.x += 1.f; F1.y += 1.f; F2.z += 1.f;
+        if (S.damping == 0.f) {   // without damping only -V P g is needed: P~ once per point
+            pk1_tilde<MAT>(F0, F1, F2, C.z, C.w, C.y * wq<E>(q), m0, m1, m2, F0, F1, F2);
+        }
+        s_F[grp][q][0] = make_float4(F0.x, F0.y, F0.z, 0.f);
+        s_F[grp][q][1] = make_float4(F1.x, F1.y, F1.z, 0.f);
+        s_F[grp][q][2] = make_float4(F2.x, F2.y, F2.z, 0.f);
+        s_R[grp][q][0] = A;
+        s_R[grp][q][1] = B;
+        s_R[grp][q][2] = make_float4(C.x, C.y * wq<E>(q), C.z, C.w);
+    }
+    __syncwarp();
+    const float kd = S.damping;
+    if (kd == 0.f) {   // f_i = -sum_q P~_q dN_qi
+#pragma unroll
+        for (int k = 0; k < NI; ++k) {
+            const int i = lane + k * G;
+            if (!active || i >= NE) continue;
+            float fx = 0.f, fy = 0.f, fz = 0.f;
+#pragma unroll (NQ <= 11 ? NQ : 1)
+            for (int q = 0; q < NQ; ++q) {
+                const float4 t0 = s_F[grp][q][0], t1 = s_F[grp][q][1], t2 = s_F[grp][q][2];
+                const float* dr = &s_dN[(q * NE + i) * 3];
+                fx -= t0.x * dr[0] + t1.x * dr[1] + t2.x * dr[2];
+                fy -= t0.y * dr[0] + t1.y * dr[1] + t2.y * dr[2];
+                fz -= t0.z * dr[0] + t1.z * dr[1] + t2.z * dr[2];
+            }
+            contrib[(size_t)eid * NE + i] = make_float4(fx, fy, fz, 0.f);
+        }
+        return;
+    }
+#pragma unroll
+    for (int k = 0; k < NI; ++k) {
+        const int i = lane + k * G;
+        if (!active || i >= NE) continue;
+        float acc[9];
+#pragma unroll
+        for (int t = 0; t < 9; ++t) acc[t] = 0.f;
+#pragma unroll (NQ <= 11 ? NQ : 1)
+        for (int q = 0; q < NQ; ++q) {
+            const float4 f0 = s_F[grp][q][0], f1 = s_F[grp][q][1], f2 = s_F[grp][q][2];
+            const float4 A = s_R[grp][q][0], B = s_R[grp][q][1], C = s_R[grp][q][2];
+            const V3 m0 = mk(A.x, A.y, A.z), m1 = mk(A.w, B.x, B.y), m2 = mk(B.z, B.w, C.x);
+            const float* dr = &s_dN[(q * NE + i) * 3];
+            const V3 dnr = mk(dr[0], dr[1], dr[2]);
+            const V3 g = mk(dot(m0, dnr), dot(m1, dnr), dot(m2, dnr));
+            float t[9];
+            material_terms<MAT>(mk(f0.x, f0.y, f0.z), mk(f1.x, f1.y, f1.z), mk(f2.x, f2.y, f2.z), g, C.z, C.w, C.y, t);
+#pragma unroll
+            for (int j = 0; j < 9; ++j) acc[j] += t[j];
+        }
+        const float4 vv = S.v[tp[i]];
+        float4 f;
+        f.x = acc[0] - kd * (acc[3] * vv.x + acc[4] * vv.y + acc[5] * vv.z);
+        f.y = acc[1] - kd * (acc[4] * vv.x + acc[6] * vv.y + acc[7] * vv.z);
+        f.z = acc[2] - kd * (acc[5] * vv.x + acc[7] * vv.y + acc[8] * vv.z);
+        f.w = 0.f;
+        contrib[(size_t)eid * NE + i] = f;
+    }
+}
+
+// Per node: the sum of its owners' element contributions in owner order (compensated in
+// mixed precision), kept in u_new (the force buffer of the explicit solver), then the
+// semi-implicit Euler update of that node (kenerl_semi_exicit_integration,
+// octopus/src/GPU/GPU_Integrator.cu:27-34; the arithmetic of k_predict kind 1).  work indexes
+// the scene's slots (one colour: every node).
+__global__ void k_explicit_gather(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work,
+                                  const float4* __restrict__ contrib, int ne, StepParams P) {
+    pdl_trigger();
+    pdl_wait();
+    const NWork wk = work[blockIdx.x];
+    if ((int)threadIdx.x >= wk.count) return;
+    const SceneDev& S = scenes[wk.scene];
+    const int slot = wk.begin + threadIdx.x;
+    const int vid = S.vids[slot];
+    const int ob = S.own_off[slot], oe = S.own_off[slot + 1];
+    const bool mixed = S.precision != 0;
+    float fx = 0.f, fy = 0.f, fz = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+    for (int o = ob; o < oe; ++o) {
+        const int packed = __ldg(S.owners + o);
+        const float4 c = contrib[(size_t)(packed >> kOwnerShift) * ne + (packed & ((1 << kOwnerShift) - 1))];
+        if (mixed) { kadd(fx, cx, c.x); kadd(fy, cy, c.y); kadd(fz, cz, c.z); }
+        else { fx += c.x; fy += c.y; fz += c.z; }
+    }
+    if (mixed) { fx -= cx; fy -= cy; fz -= cz; }
+    S.u_new[vid] = make_float4(fx, fy, fz, 0.f);
+    const float dt = P.dt;
+    float4 u = S.u[vid], v = S.v[vid];
+    const float w = 1.f / S.y[vid].w;
+    S.u_last[vid] = u;
+    v.x += (S.gx + fx * w) * dt; v.y += (S.gy + fy * w) * dt; v.z += (S.gz + fz * w) * dt;
+    u.x += v.x * dt; u.y += v.y * dt; u.z += v.z * dt;
+    S.v[vid] = v;
+    S.u[vid] = u;
+    if (!isfinite(u.x + u.y + u.z + v.x + v.y + v.z)) atomicOr(S.status, kStatusNonFinite);
+}
+
 template <int E>
 __global__ void __launch_bounds__(kBlock) k_element_diag(const SceneDev* __restrict__ scenes, int scene, int kind,
                                                          int material, float* __restrict__ out) {
@@ -1775,6 +1960,35 @@ void launch_xpbd(int element, int material, bool raw, const SceneDev* scenes, co
         case 8: xpbd_form<8>(material, raw, scenes, work, n_work, P, st); break;
         case 9: xpbd_form<9>(material, raw, scenes, work, n_work, P, st); break;
     }
+}
+
+namespace {
+template <int E>
+void explicit_mat(int mat, const SceneDev* scenes, int n_elements, float4* contrib, const StepParams& P, cudaStream_t st) {
+    const int grid = (n_elements + kBlock / XpbdLanes<E>::G - 1) / (kBlock / XpbdLanes<E>::G);
+    switch (mat) {
+        case 0: launch_pdl(k_explicit_elem<E, 0>, grid, kBlock, 0, st, scenes, n_elements, contrib, P); break;
+        case 1: launch_pdl(k_explicit_elem<E, 1>, grid, kBlock, 0, st, scenes, n_elements, contrib, P); break;
+        case 2: launch_pdl(k_explicit_elem<E, 2>, grid, kBlock, 0, st, scenes, n_elements, contrib, P); break;
+        default: launch_pdl(k_explicit_elem<E, 3>, grid, kBlock, 0, st, scenes, n_elements, contrib, P); break;
+    }
+}
+}  // namespace
+
+void launch_explicit_force(int element, int material, const SceneDev* scene, int n_elements, float4* contrib,
+                           const NWork* slots, int n_slots, const StepParams& P, cudaStream_t st) {
+    if (n_elements <= 0) return;
+    switch (element) {
+        case 3: explicit_mat<3>(material, scene, n_elements, contrib, P, st); break;
+        case 6: explicit_mat<6>(material, scene, n_elements, contrib, P, st); break;
+        case 7: explicit_mat<7>(material, scene, n_elements, contrib, P, st); break;
+        case 8: explicit_mat<8>(material, scene, n_elements, contrib, P, st); break;
+        case 9: explicit_mat<9>(material, scene, n_elements, contrib, P, st); break;
+        default: return;
+    }
+    if (n_slots > 0)
+        launch_pdl(k_explicit_gather, n_slots, kNodeChunk, 0, st, scene, slots, (const float4*)contrib,
+                   element == 3 ? 4 : element == 6 ? 8 : element == 7 ? 10 : element == 8 ? 20 : 27, P);
 }
 
 int xpbd_elements_per_block(int element) {

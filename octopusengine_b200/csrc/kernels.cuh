@@ -15,6 +15,12 @@ void prepare_vertex(int element, int material);
 void launch_vertex(int element, int material, const SceneDev* scenes, const VWork* work, int n_work, int tpv, int mode,
                    const StepParams& P, double* red, cudaStream_t st);
 void launch_commit(const SceneDev* scenes, const VWork* work, int n_work, cudaStream_t st);
+// Explicit sub-step without the constraints: the element-centric force pass (per-(element,
+// local node) contributions into contrib, n_elements x NE float4), then per node the sum over
+// its owners into u_new and the semi-implicit Euler update (slots: node chunks over the
+// scene's slots).
+void launch_explicit_force(int element, int material, const SceneDev* scene, int n_elements, float4* contrib,
+                           const NWork* slots, int n_slots, const StepParams& P, cudaStream_t st);
 // kind 0: VBD predictor, kind 1: semi-implicit Euler (use_force: add the force in u_new)
 void launch_predict(const SceneDev* scenes, const NWork* work, int n_work, int kind, int use_force, int chebyshev,
                     const StepParams& P, cudaStream_t st);

@@ -181,6 +181,7 @@ struct oct_scene {
     double* d_red = nullptr;        // 4 doubles of reduction scratch
     float* d_io = nullptr;          // n_nodes x 3 floats: node state in and out (allocated on first use)
     float* d_diag = nullptr;        // per-element diagnostics output (allocated on first use)
+    float4* d_contrib = nullptr;    // explicit: per-(element, local node) force contributions
     // scripted effects (oct_scene_add_effect): host copy of the device slots
     EffectDev effects[kMaxEffects];
     EffectDev* d_effects = nullptr;
@@ -778,6 +779,7 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     s->pending_host = s->has_v0 && d->solver == OCT_SOLVER_VBD ? 1 : 0;
     if ((st = upload(c, s->mem, s->d_pending, std::vector<int>{s->pending_host}))) return st;
     if ((st = s->mem.alloc(s->d_red, 4))) return st;
+    if (d->solver == OCT_SOLVER_EXPLICIT && (st = s->mem.alloc(s->d_contrib, (size_t)E * NE))) return st;
 
     // work tables
     if ((st = build_vertex_work(s))) return st;
@@ -917,8 +919,9 @@ void explicit_substep(oct_scene* s, float dt) {
     oct_ctx* c = s->ctx;
     cudaStream_t st = c->stream;
     StepParams P = base_params(c, dt);
-    launch_vertex(s->element, s->material, s->d_scene, s->d_vwork, s->vwork_off[1], s->tpv, 2, P, nullptr, st);
-    launch_predict(s->d_scene, s->d_nwork, s->n_nwork, 1, 1, 0, P, st);
+    // element-centric force pass, then per node the sum over its owners and the semi-implicit
+    // Euler update (GPU_FEM_Explicit::step then GPU_SemiExplicit's integration)
+    launch_explicit_force(s->element, s->material, s->d_scene, s->n_elements, s->d_contrib, s->d_nwork, s->n_nwork, P, st);
     c->launches += 2;
     if (s->n_fixed) { launch_constraints(s->d_scene, s->d_fwork, s->n_fwork, 0, st); c->launches++; }
     enqueue_effects(s, dt, st);
@@ -1042,6 +1045,7 @@ oct_status oct_scene_footprint(const oct_scene_desc* d, size_t* bytes) {
     b += E * ne * sizeof(int) * 2 + E * nq * 3 * sizeof(float4);   // topology, owners, quadrature records
     b += E * ne * (size_t)entry_words(ne) * sizeof(float);                  // owner entries
     b += (ne == 4 ? 4 : 1) * E * 3 * sizeof(float4);                        // distinct records, at most
+    if (d->solver == OCT_SOLVER_EXPLICIT) b += E * ne * sizeof(float4);     // explicit force contributions
     b += (N / 16 + 64) * sizeof(VWork) + (N / 256 + 8) * 2 * sizeof(NWork) + (size_t)std::max(d->n_fixed, 0) * sizeof(int);
     b += 4096;   // descriptors and reduction scratch
     *bytes = b;
