@@ -108,7 +108,8 @@ typedef struct oct_scene_desc {
     float box_min[3], box_max[3];
     int32_t threads_per_vertex;     /* 0 = measured default per element, -1 = one lane per
                                        (vertex, owner) pair packed into warps, 1..32 = lanes per
-                                       vertex (power of two) */
+                                       vertex (power of two; a colour whose vertices average
+                                       more than 8 owners per lane gets wider groups) */
     int32_t xpbd_version;           /* OCT_XPBD_* (default OCT_XPBD_OPTISHARED) */
     float mg_linear;                /* multigrid VBD for P2 / Q2 (MG_VBD_FEM,
                                        octopus/include/Dynamic/VBD/MG_VertexBlockDescent.h:52-74):
@@ -249,7 +250,8 @@ oct_status oct_scene_get_mapping(oct_scene* s, int32_t* threads_per_vertex);
 /* Mapping autotuner (new): for each element type among the VBD and explicit scenes (XPBD
  * scenes are skipped), times one colour sweep of all its scenes under every candidate mapping
  * (packed pairs when every scene has owner entries and at most 32 owners per vertex, 1, 2, 4,
- * 8, 16, 32 lanes per vertex) and sets the fastest on those scenes.  The timed sweeps write only the Jacobi
+ * 8, 16, 32 lanes per vertex; best of three timings each) and sets the fastest on those
+ * scenes, keeping the measured default unless another mapping is at least 3 % faster.  The timed sweeps write only the Jacobi
  * scratch buffer, so positions and velocities are unchanged.  chosen (may be NULL): per
  * element id the mapping picked (-1 packed), 0 for element types absent.  Run it before
  * oct_batch_create; it leaves no batch behind. */

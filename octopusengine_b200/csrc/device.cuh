@@ -105,7 +105,8 @@ struct VWork {
     int pair_base;
     unsigned heads;   // packed items: bit p set when pair p starts a new vertex
     int n_pairs;      // packed items: number of (vertex, owner) pairs
-    int pad0, pad1;
+    int tpv;          // lane-group items: lanes per vertex of this item; 0 = the launch's
+    int pad1;
 };
 
 // Owner entries: one per (vertex, owner) pair in slot order, contiguous per vertex (and per

@@ -733,10 +733,11 @@ __global__ void __launch_bounds__(kBlock, LaneMinBlocks<E>::value) k_vertex(cons
     pdl_wait();
 
     const int lane = threadIdx.x & 31;
-    const int glane = lane & (tpv - 1);           // lane within the vertex group
-    const int group = threadIdx.x / tpv;          // vertex index within the block
     for (int w = blockIdx.x; w < n_work; w += gridDim.x) {
         const VWork wk = work[w];
+        const int t = wk.tpv ? wk.tpv : tpv;    // lanes per vertex of this item (block-uniform)
+        const int glane = lane & (t - 1);        // lane within the vertex group
+        const int group = threadIdx.x / t;       // vertex index within the block
         const SceneDev& S = scenes[wk.scene];
         const bool valid = group < wk.count;
         const int slot = wk.slot_begin + group;
@@ -767,7 +768,7 @@ __global__ void __launch_bounds__(kBlock, LaneMinBlocks<E>::value) k_vertex(cons
                     float4 cur[EW / 4];
 #pragma unroll
                     for (int j = 0; j < EW / 4; ++j) cur[j] = nxt[j];
-                    const int on = o + tpv;
+                    const int on = o + t;
                     if (on < oe) {
 #pragma unroll
                         for (int j = 0; j < EW / 4; ++j) nxt[j] = ld_hint(base + (size_t)on * (EW / 4) + j, stream);
@@ -776,14 +777,14 @@ __global__ void __launch_bounds__(kBlock, LaneMinBlocks<E>::value) k_vertex(cons
                     o = on;
                 }
             } else {
-                for (int o = ob + glane; o < oe; o += tpv) owner_terms<E, MAT>(S, __ldg(S.owners + o), s_dN, mixed, acc, cmp);
+                for (int o = ob + glane; o < oe; o += t) owner_terms<E, MAT>(S, __ldg(S.owners + o), s_dN, mixed, acc, cmp);
             }
             if (mixed) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) acc[k] -= cmp[k];
             }
         }
-        for (int off = tpv >> 1; off > 0; off >>= 1) {
+        for (int off = t >> 1; off > 0; off >>= 1) {
 #pragma unroll
             for (int k = 0; k < 9; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], off);
         }
