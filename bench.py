@@ -647,8 +647,8 @@ def vertex_kernel_label(group, scenes):
     if tpv == -1:
         return "k_vertex_packed<%d,%d> (VBD colour sweep, element %d, one lane per (vertex, owner) pair)" % (
             group["element"], group["material"], group["element"])
-    return "k_vertex<%d,%d> (VBD colour sweep, element %d, %d lanes per vertex)" % (
-        group["element"], group["material"], group["element"], tpv)
+    return "k_vertex<%d,%d> (VBD colour sweep, element %d, %d lanes per vertex, wider on colours of more than %d owners per lane)" % (
+        group["element"], group["material"], group["element"], tpv, 8)
 
 
 def parity_sample(scenes, specs, positions, frames, iterations, substeps, frame_dt, threads):

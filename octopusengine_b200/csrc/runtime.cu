@@ -299,7 +299,7 @@ int measured_tpv(int element) {
     switch (element) {
         case kTetra: return 4;
         case kHexa: return 4;
-        case kTetra10: return 2;
+        case kTetra10: return 1;   // corner colours widen to 4 lanes (kOwnersPerLane)
         default: return 0;
     }
 }
@@ -643,8 +643,9 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
         max_valence = std::max(max_valence, own_off[sl + 1] - own_off[sl]);
     }
     // default mapping (per-colour sweep times measured on the batched workload): P1 tetrahedra
-    // and Q1 hexahedra use 4 lanes per vertex, P2 tetrahedra 2, each lane looping over a share
-    // of the vertex's owners; the other elements one lane per (vertex, owner) pair packed into
+    // and Q1 hexahedra use 4 lanes per vertex, P2 tetrahedra 1 (4 on the corner colours, by
+    // kOwnersPerLane; P2 sweep 1.672 ms against 1.730 ms with 2), each lane looping over a
+    // share of the vertex's owners; the other elements one lane per (vertex, owner) pair packed into
     // warps; vertices with more than 32 owners fall back to a lane group per vertex
     if (d->threads_per_vertex == 0) s->tpv = measured_tpv(d->element);
     if (s->tpv == 0 && max_valence > 32) s->tpv = max_valence > 64 ? 32 : default_tpv(d->element);
