@@ -166,3 +166,17 @@ def test_high_valence_fallback(ctx):
         s.step(0.01, 1)
         ref.step(0.01, 1)
     assert rel_err(s.get_position(), ref.get(0)) < 1e-5
+
+
+@pytest.mark.parametrize("cells", [(6, 4, 4), (12, 8, 8)])
+def test_p2_entry_forms_with_many_records(ctx, cells):
+    """P2 scenes whose owner entries index many distinct quadrature records (a Young modulus per
+    element: 576 and 4608 records) match the FP64 oracle."""
+    X, T = O.beam_mesh(O.TETRA10, cells, (cells[0] * 0.1, cells[1] * 0.1, cells[2] * 0.1))
+    E = np.exp(np.random.default_rng(8).uniform(np.log(1e4), np.log(1e6), len(T))).astype(np.float32)
+    s, o32, o64, mesh = pair(ctx, O.TETRA10, cells=cells, size=(cells[0] * 0.1, cells[1] * 0.1, cells[2] * 0.1),
+                             iterations=4, young_per_element=E)
+    s.step(1 / 60, 1)
+    o32.step(1 / 60, 1)
+    o64.step(1 / 60, 1)
+    check_parity(s.get_position(), o32, o64, mesh["X"], ("P2 entries", cells))
