@@ -65,6 +65,7 @@ struct SceneDev {
     const int* owners;  // packed (eid << 5) | r
     const int* fixed;   // n_fixed node ids
     const int* fixed_group;            // n_fixed rigid-group indices
+    const int* fix_of;                 // explicit: per node its rigid group if fixed, else -1 (or null)
     const float* fix;                  // kFixGroups x 16: com (3), offset (3), rotation (9, column-major), pad
     int n_nodes, n_elements, n_fixed, element;
     int eq_stride;                     // records per element: NQ, or 1 for affine elements

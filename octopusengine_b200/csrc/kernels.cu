@@ -881,6 +881,22 @@ __global__ void k_chebyshev(const SceneDev* __restrict__ scenes, const NWork* __
 
 // Fixed nodes (kernel_constraint_fix, GPU_Constraint.cu:8-20) then, if enabled, the box
 // clamp of free nodes (kernel_constraint_box_limit, :80-92).  One block per scene chunk.
+// Fixation of node id to rigid group g (kernel_fix_constraint, GPU_Constraint.cu:8-20):
+// position com + offset + R (X - com), velocity 0, mask 0.
+__device__ __forceinline__ void fix_node(const SceneDev& S, int id, int g) {
+    const float* G = S.fix + 16 * g;   // com, offset, rotation
+    const float4 X = S.X[id];
+    const float dx = X.x - G[0], dy = X.y - G[1], dz = X.z - G[2];
+    const float* R = G + 6;
+    const float rx = R[0] * dx + R[3] * dy + R[6] * dz;
+    const float ry = R[1] * dx + R[4] * dy + R[7] * dz;
+    const float rz = R[2] * dx + R[5] * dy + R[8] * dz;
+    const float tx = (G[3] + G[0]) + rx, ty = (G[4] + G[1]) + ry, tz = (G[5] + G[2]) + rz;
+    S.u[id] = make_float4(tx - X.x, ty - X.y, tz - X.z, 0.f);
+    S.v[id] = make_float4(0.f, 0.f, 0.f, 0.f);
+    S.mask[id] = 0;
+}
+
 __global__ void k_constraints(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work, int n_work, int box_pass) {
     pdl_trigger();
     pdl_wait();
@@ -889,18 +905,7 @@ __global__ void k_constraints(const SceneDev* __restrict__ scenes, const NWork* 
     const SceneDev& S = scenes[wk.scene];
     const int k = wk.begin + threadIdx.x;
     if (!box_pass) {
-        const int id = S.fixed[k];
-        const float* G = S.fix + 16 * S.fixed_group[k];   // com, offset, rotation
-        const float4 X = S.X[id];
-        const float dx = X.x - G[0], dy = X.y - G[1], dz = X.z - G[2];
-        const float* R = G + 6;
-        const float rx = R[0] * dx + R[3] * dy + R[6] * dz;
-        const float ry = R[1] * dx + R[4] * dy + R[7] * dz;
-        const float rz = R[2] * dx + R[5] * dy + R[8] * dz;
-        const float tx = (G[3] + G[0]) + rx, ty = (G[4] + G[1]) + ry, tz = (G[5] + G[2]) + rz;
-        S.u[id] = make_float4(tx - X.x, ty - X.y, tz - X.z, 0.f);
-        S.v[id] = make_float4(0.f, 0.f, 0.f, 0.f);
-        S.mask[id] = 0;
+        fix_node(S, S.fixed[k], S.fixed_group[k]);
     } else {
         if (S.mask[k] == 0) return;
         const float4 X = S.X[k];
@@ -1544,7 +1549,8 @@ __global__ void __launch_bounds__(kBlock) k_explicit_elem(const SceneDev* __rest
 // Per node: the sum of its owners' element contributions in owner order (compensated in
 // mixed precision), kept in u_new (the force buffer of the explicit solver), then the
 // semi-implicit Euler update of that node (kenerl_semi_exicit_integration,
-// octopus/src/GPU/GPU_Integrator.cu:27-34; the arithmetic of k_predict kind 1).  work indexes
+// octopus/src/GPU/GPU_Integrator.cu:27-34; the arithmetic of k_predict kind 1) and, for a
+// fixed node, its fixation (fix_node, as k_constraints).  work indexes
 // the scene's slots (one colour: every node).
 __global__ void k_explicit_gather(const SceneDev* __restrict__ scenes, const NWork* __restrict__ work,
                                   const float4* __restrict__ contrib, int ne, StepParams P) {
@@ -1575,6 +1581,12 @@ __global__ void k_explicit_gather(const SceneDev* __restrict__ scenes, const NWo
     S.v[vid] = v;
     S.u[vid] = u;
     if (!isfinite(u.x + u.y + u.z + v.x + v.y + v.z)) atomicOr(S.status, kStatusNonFinite);
+    // then the fixation of the sub-step (GPU_SemiExplicit::step applies the constraints after
+    // the integration): fixed nodes are set to their group's target
+    if (S.fix_of) {
+        const int g = S.fix_of[vid];
+        if (g >= 0) fix_node(S, vid, g);
+    }
 }
 
 template <int E>

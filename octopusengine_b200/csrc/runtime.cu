@@ -683,6 +683,13 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     h.u = u; h.u_last = ul; h.y = y; h.v = v; h.u_new = un; h.prev1 = p1; h.prev2 = p2; h.mask = maskd; h.X = Xd;
     h.topo = topod; h.eq = eqd; h.vids = vidsd; h.own_off = offd; h.owners = ownd; h.fixed = fixd;
     h.fixed_group = fgd; h.fix = s->d_fix;
+    if (d->solver == OCT_SOLVER_EXPLICIT && s->n_fixed) {   // the explicit update applies the fixation itself
+        std::vector<int32_t> fix_of(N, -1);
+        for (int k = 0; k < s->n_fixed; ++k) fix_of[s->fixed[k]] = s->fixed_group[k];
+        int* fod;
+        if ((st = upload(c, s->mem, fod, fix_of))) return st;
+        h.fix_of = fod;
+    }
     h.n_nodes = N; h.n_elements = E; h.n_fixed = s->n_fixed; h.element = d->element;
     h.damping = d->damping;
     h.gx = d->gravity[0]; h.gy = d->gravity[1]; h.gz = d->gravity[2];
@@ -936,8 +943,7 @@ void explicit_substep(oct_scene* s, float dt) {
     // element-centric force pass, then per node the sum over its owners and the semi-implicit
     // Euler update (GPU_FEM_Explicit::step then GPU_SemiExplicit's integration)
     launch_explicit_force(s->element, s->material, s->d_scene, s->n_elements, s->d_contrib, s->d_nwork, s->n_nwork, P, st);
-    c->launches += 2;
-    if (s->n_fixed) { launch_constraints(s->d_scene, s->d_fwork, s->n_fwork, 0, st); c->launches++; }
+    c->launches += 2;   // the fixation runs inside the update kernel (SceneDev::fix_of)
     enqueue_effects(s, dt, st);
     if (s->box) { launch_constraints(s->d_scene, s->d_nwork, s->n_nwork, 1, st); c->launches++; }
 }
@@ -1059,7 +1065,7 @@ oct_status oct_scene_footprint(const oct_scene_desc* d, size_t* bytes) {
     b += E * ne * sizeof(int) * 2 + E * nq * 3 * sizeof(float4);   // topology, owners, quadrature records
     b += E * ne * (size_t)entry_words(ne) * sizeof(float);                  // owner entries
     b += (ne == 4 ? 4 : 1) * E * 3 * sizeof(float4);                        // distinct records, at most
-    if (d->solver == OCT_SOLVER_EXPLICIT) b += E * ne * sizeof(float4);     // explicit force contributions
+    if (d->solver == OCT_SOLVER_EXPLICIT) b += E * ne * sizeof(float4) + N * sizeof(int);   // contributions, fixation map
     b += (N / 16 + 64) * sizeof(VWork) + (N / 256 + 8) * 2 * sizeof(NWork) + (size_t)std::max(d->n_fixed, 0) * sizeof(int);
     b += 4096;   // descriptors and reduction scratch
     *bytes = b;
