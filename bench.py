@@ -728,7 +728,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched",
-                    choices=["batched", "p2", "cfg1", "cube_p3", "cube_q2", "xpbd_p2", "explicit_p2", "served"])
+                    choices=["batched", "p2", "cfg1", "cube_p3", "cube_q2", "xpbd_p2", "explicit_p2", "served",
+                             "xpbd_batched"])
     ap.add_argument("--rates", default="4,8,16", help="served: Poisson arrival rates (requests/s)")
     ap.add_argument("--serve-seconds", type=float, default=20.0, help="served: arrival window per rate")
     ap.add_argument("--seed", type=int, default=2024)
@@ -752,6 +753,31 @@ def main():
     threads = os.cpu_count() or 1
     if args.workload in SOLVER_WORKLOADS:
         bench_solver(args, world, rank, local, threads)
+        return
+    if args.workload == "xpbd_batched":   # the batched workload's scenes as XPBD scenes, alone
+        if args.impl == "reference" or rank != 0:
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference's XPBD path is GPU-only; "
+                                  "its CPU VBD path is timed by the batched workload"}))
+            return
+        import torch
+        torch.cuda.set_device(local)
+        import octopusengine_b200 as ob
+        specs, _, _, _ = workload_specs("batched", args.seed)
+        if args.scenes > 0:
+            specs = specs[:args.scenes]
+        from octopusengine_b200 import capi
+        import ctypes as C
+        ctx = ob.Context(local, 0)
+        stream_ptr = C.c_void_p()
+        capi.lib().oct_ctx_stream(ctx.handle, C.byref(stream_ptr))
+        stream = torch.cuda.ExternalStream(stream_ptr.value, device=local)
+        line = batched_xpbd(ctx, specs, args.seed, stream, threads, warmup=args.warmup, steps=args.steps)
+        ctx.close()
+        print(json.dumps({"metric": "element_projections_per_s", "value": line["value"], "unit": line["unit"],
+                          "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                          "ms_per_step": line["ms_per_frame"], "config": {"workload": "xpbd_batched",
+                          "scenes": len(specs)}, "xpbd_batched": line}))
         return
     if args.workload == "served":
         if args.impl == "reference" or rank != 0:

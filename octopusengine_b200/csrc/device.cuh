@@ -79,6 +79,7 @@ struct SceneDev {
     EffectDev* effects;                // kMaxEffects slots (scene memory)
     int* status;                       // per-scene failure flags: kStatusTimeout, kStatusNonFinite
     const int* elems;                  // XPBD: element ids sorted by colour
+    const int* etopo;                  // XPBD: their topology in the same order (NE ids per slot)
     float global_damping;              // XPBD velocity damping (GPU_PBD global_damping)
 };
 

@@ -1238,8 +1238,8 @@ __global__ void __launch_bounds__(kBlock) k_xpbd(const SceneDev* __restrict__ sc
     const XWork wk = work[blockIdx.x];   // GPB elements of one scene's colour
     const bool active = grp < wk.count;   // no early exit: every lane takes part in the shuffles
     const SceneDev& S = scenes[wk.scene];
-    const int eid = active ? S.elems[wk.begin + grp] : 0;
-    const int* tp = S.topo + (size_t)eid * NE;
+    const int eid = active ? S.elems[wk.begin + grp] : 0;   // for the quadrature records only
+    const int* tp = S.etopo + (size_t)(active ? wk.begin + grp : 0) * NE;
     int vid[NI];
     float4 u[NI];
     float w[NI];

@@ -175,6 +175,7 @@ struct oct_scene {
     NWork* d_fwork = nullptr;
     int n_fwork = 0;
     int* d_elems = nullptr;         // XPBD: colour-sorted element ids
+    int* d_etopo = nullptr;         // XPBD: their topology in colour order
     std::vector<int> elem_off;
     XWork* d_xwork = nullptr;       // XPBD: block work items of the scene's own steps
     std::vector<int> xwork_off;     // per colour: [xwork_off[c], xwork_off[c+1])
@@ -592,6 +593,12 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
         std::vector<int32_t> flat;
         for (auto& v : elems_by_color) { flat.insert(flat.end(), v.begin(), v.end()); s->elem_off.push_back((int)flat.size()); }
         if ((st = upload(c, s->mem, s->d_elems, flat))) return st;
+        // the topology in colour order: a block's node ids follow from its work item directly,
+        // one dependent load fewer before the gathers (element ids only index the records)
+        std::vector<int32_t> etopo(flat.size() * (size_t)NE);
+        for (size_t k = 0; k < flat.size(); ++k)
+            std::copy(d->topology + (size_t)flat[k] * NE, d->topology + (size_t)(flat[k] + 1) * NE, etopo.begin() + k * NE);
+        if ((st = upload(c, s->mem, s->d_etopo, etopo))) return st;
         std::vector<XWork> xw;
         s->xwork_off.assign(1, 0);
         for (int k = 0; k + 1 < (int)s->elem_off.size(); ++k) {
@@ -789,6 +796,7 @@ oct_status build_scene(oct_ctx* c, const oct_scene_desc* d, oct_scene* s) {
     if ((st = upload(c, s->mem, s->d_effects, std::vector<EffectDev>(s->effects, s->effects + kMaxEffects)))) return st;
     h.effects = s->d_effects;
     h.elems = s->d_elems;
+    h.etopo = s->d_etopo;
     h.global_damping = s->global_damping;
     if ((st = upload(c, s->mem, s->d_status, std::vector<int>{0}))) return st;
     h.status = s->d_status;
@@ -1067,6 +1075,7 @@ oct_status oct_scene_footprint(const oct_scene_desc* d, size_t* bytes) {
     b += (ne == 4 ? 4 : 1) * E * 3 * sizeof(float4);                        // distinct records, at most
     if (d->solver == OCT_SOLVER_EXPLICIT) b += E * ne * sizeof(float4) + N * sizeof(int);   // contributions, fixation map
     b += (N / 16 + 64) * sizeof(VWork) + (N / 256 + 8) * 2 * sizeof(NWork) + (size_t)std::max(d->n_fixed, 0) * sizeof(int);
+    if (d->solver == OCT_SOLVER_XPBD) b += E * (ne + 1) * sizeof(int);   // colour-sorted element ids and topology
     b += 4096;   // descriptors and reduction scratch
     *bytes = b;
     return OCT_OK;
