@@ -1220,8 +1220,13 @@ template <int G> __device__ __forceinline__ float group_sum(float v) {
     return v;
 }
 
-template <int E, int MAT, bool RAW>
-__global__ void __launch_bounds__(kBlock) k_xpbd(const SceneDev* __restrict__ scenes, const XWork* __restrict__ work,
+// MINB: resident blocks per SM the kernel is compiled for.  1 (96 registers for P2, 5 blocks)
+// serves launches of under a wave (one scene's colour: per-element latency decides); 8 (64
+// registers) serves batched launches of several waves, whose time is set by how many elements
+// are in flight: the 256-scene XPBD frame 17.05 -> 15.65 ms, against a single P2 scene's frame
+// 0.889 -> 0.989 ms with 6 blocks.
+template <int E, int MAT, bool RAW, int MINB>
+__global__ void __launch_bounds__(kBlock, MINB) k_xpbd(const SceneDev* __restrict__ scenes, const XWork* __restrict__ work,
                                                  StepParams P) {
     constexpr int NE = ElemT<E>::NE, NQ = ElemT<E>::NQ, G = XpbdLanes<E>::G, GPB = kBlock / G;
     constexpr int NI = (NE + G - 1) / G;   // nodes per lane
@@ -1802,16 +1807,27 @@ void vertex_mat(int mat, const SceneDev* scenes, const VWork* work, int n_work, 
     }
 }
 
+template <int E, bool RAW, int MINB>
+void xpbd_launch(int mat, const SceneDev* scenes, const XWork* work, int n_work, const StepParams& P, cudaStream_t st) {
+    switch (mat) {
+        case 0: launch_pdl(k_xpbd<E, 0, RAW, MINB>, n_work, kBlock, 0, st, scenes, work, P); break;
+        case 1: launch_pdl(k_xpbd<E, 1, RAW, MINB>, n_work, kBlock, 0, st, scenes, work, P); break;
+        case 2: launch_pdl(k_xpbd<E, 2, RAW, MINB>, n_work, kBlock, 0, st, scenes, work, P); break;
+        case 3: launch_pdl(k_xpbd<E, 3, RAW, MINB>, n_work, kBlock, 0, st, scenes, work, P); break;
+        case 4: launch_pdl(k_xpbd<E, 4, RAW, MINB>, n_work, kBlock, 0, st, scenes, work, P); break;
+        default: launch_pdl(k_xpbd<E, 5, RAW, MINB>, n_work, kBlock, 0, st, scenes, work, P); break;
+    }
+}
 template <int E, bool RAW>
 void xpbd_mat(int mat, const SceneDev* scenes, const XWork* work, int n_work, const StepParams& P, cudaStream_t st) {
-    switch (mat) {
-        case 0: launch_pdl(k_xpbd<E, 0, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
-        case 1: launch_pdl(k_xpbd<E, 1, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
-        case 2: launch_pdl(k_xpbd<E, 2, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
-        case 3: launch_pdl(k_xpbd<E, 3, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
-        case 4: launch_pdl(k_xpbd<E, 4, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
-        default: launch_pdl(k_xpbd<E, 5, RAW>, n_work, kBlock, 0, st, scenes, work, P); break;
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     }
+    if (n_work > 5 * sms) xpbd_launch<E, RAW, 8>(mat, scenes, work, n_work, P, st);   // more than a wave at 5 blocks/SM
+    else xpbd_launch<E, RAW, 1>(mat, scenes, work, n_work, P, st);
 }
 template <int E>
 void xpbd_form(int mat, bool raw, const SceneDev* scenes, const XWork* work, int n_work, const StepParams& P,
