@@ -12,8 +12,8 @@ metric: vertex-iterations/s = sum over scenes of free nodes x iterations x sub-s
 step, / time.  Also reported: the plain single-scene drop-in path (each scene stepped on
 its own, FP32, one launch per colour, no graph) on the same scenes and GPU, p50/p99 step
 latency, the end-to-end number through the C ABI with host buffers, the roofline of the
-dominant kernel (SURVEY 8(d) algorithmic flops and bytes; the executed-flop rate beside
-them), the reference CPU VBD path timed on the host cores (one thread, as the reference runs;
+dominant kernel (algorithmic flops and bytes of the reference algorithm: Jx, F, dF/dx, PK1,
+the six symmetric Hessian blocks and their assembly; the executed-flop rate beside them), the reference CPU VBD path timed on the host cores (one thread, as the reference runs;
 all threads as an extension), the timed run's error against the FP64 oracle on a sample of
 its scenes (`parity`), and, on the same GPU, config 2 as a single scene (`p2_single`), config
 3's P3 and Q2 cubes at 32^3 cells (`cube`), the same 256 beams as XPBD scenes in one batch
@@ -951,7 +951,7 @@ def main():
                 "kernel": vertex_kernel_label(dom, scenes),
                 "launch_ms": per_launch_s * 1e3,
                 "algorithmic": {"bytes_per_launch": bytes_per_launch, "flops_per_launch": flops_per_launch,
-                                "per_unit": "SURVEY 8(d): 18 n_e + 480 flops per (vertex, owner, quadrature point); "
+                                "per_unit": "reference algorithm: 18 n_e + 480 flops per (vertex, owner, quadrature point); "
                                             "40 B per node + (4 n_e + 40 Q) B per element per sweep"},
                 "binding_roof": "fp32",
                 "fp32": {"achieved_tflops": achieved_tflops, "peak_tflops": fp32_peak.value,
